@@ -1,0 +1,221 @@
+/*
+ * claw2.h -- C ABI of the B200 (sm_100a) Clawpack 2D wave-propagation step.
+ *
+ * This header is the drop-in boundary for PyClaw's 2D classic solver.  In the
+ * reference, ClawSolver2D.step_hyperbolic (src/pyclaw/classic/solver.py:498-547)
+ * hands the ghosted state array qbc to the f2py module classic2:
+ *
+ *     self.qbc, cfl = self.fmod.step2(maxm, num_ghost, mx, my, qold, self.qbc,
+ *                                     self.auxbc, dx, dy, self.dt, self._method,
+ *                                     self._mthlim, aux1, aux2, aux3, work,
+ *                                     self.fwave, rpn2, rpt2)
+ *
+ * (solver.py:537-539; split mode calls step2ds twice, :525-533).  Every entry
+ * point below names the reference routine it replaces.  All functions are
+ * plain C: integers, doubles, and untyped pointers.  Device pointers are CUDA
+ * global-memory pointers on the current device; `stream` is a cudaStream_t
+ * passed as void* (NULL = legacy default stream).  Nothing here aborts the
+ * process: every call returns a claw2 status code (0 = success).
+ *
+ * Two memory layouts are used:
+ *
+ *  - "reference layout": the Fortran-ordered ghosted array of the reference,
+ *    qbc(num_eqn, 1-g:mx+g, 1-g:my+g), i.e. element (m,i,j) (0-based m, padded
+ *    i in [0,mx+2g), padded j in [0,my+2g)) lives at m + num_eqn*(i + (mx+2g)*j).
+ *    Used by the claw2_ref_* and claw2_session_* entry points.
+ *
+ *  - "device layout": one plane per component, rows along x, with a padded row
+ *    pitch; element (m,i,j) lives at m*plane + j*ld + i (padded i, j as above).
+ *    claw2_get_layout() returns ld/plane.  Used by every device-resident entry
+ *    point (claw2_fill_ghosts, claw2_step, claw2_advance).
+ */
+#ifndef CLAW2_H
+#define CLAW2_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CLAW2_ABI_VERSION 1
+#define CLAW2_MAX_EQN 8
+#define CLAW2_MAX_WAVES 8
+#define CLAW2_MAX_PARAMS 8
+#define CLAW2_NUM_GHOST 2
+
+/* ---- status codes ------------------------------------------------------ */
+enum claw2_status {
+    CLAW2_OK = 0,
+    CLAW2_ERR_INVALID = 1,        /* bad problem description or argument        */
+    CLAW2_ERR_UNSUPPORTED = 2,    /* valid in the reference, not built here      */
+    CLAW2_ERR_CUDA = 3,           /* a CUDA runtime call failed                  */
+    CLAW2_ERR_CFL = 4,            /* fixed dt and CFL > cfl_max ("giving up")    */
+    CLAW2_ERR_MAX_STEPS = 5,      /* max_steps reached before tend               */
+    CLAW2_ERR_NONFINITE = 6,      /* NaN/Inf or non-physical state produced      */
+    CLAW2_ERR_TIMEOUT = 7,        /* a bounded device wait gave up               */
+    CLAW2_ERR_NOMEM = 8,          /* allocation failed                           */
+    CLAW2_ERR_SIZE = 9            /* size beyond a documented maximum            */
+};
+
+/* ---- Riemann solvers (solver.rp in the reference; clawpack.riemann modules) */
+enum claw2_rp {
+    CLAW2_RP_ACOUSTICS = 1,       /* rp2_acoustics: q=(p,u,v); params rho,bulk,cc,zz  */
+    CLAW2_RP_VC_ACOUSTICS = 2,    /* rp2_vc_acoustics: q=(p,u,v), aux=(rho,c)         */
+    CLAW2_RP_EULER_4WAVE = 3,     /* rp2_euler_4wave: q=(rho,rhou,rhov,E); gamma,gamma1 */
+    CLAW2_RP_EULER_5WAVE = 4,     /* rp2_euler_5wave: + tracer; gamma,gamma1          */
+    CLAW2_RP_SHALLOW_ROE = 5      /* rp2_shallow_roe_with_efix: q=(h,hu,hv); grav     */
+};
+
+/* ---- boundary conditions (pyclaw.BC, src/pyclaw/solver.py:12-18) ------- */
+enum claw2_bc {
+    CLAW2_BC_CUSTOM = 0,          /* ghost cells are filled by the caller        */
+    CLAW2_BC_EXTRAP = 1,
+    CLAW2_BC_PERIODIC = 2,
+    CLAW2_BC_WALL = 3
+};
+
+/*
+ * Problem description.  Mirrors what the reference packs into method(7) and
+ * mthlim(num_waves) (ClawSolver.set_method / set_mthlim,
+ * src/pyclaw/classic/solver.py:167-198) plus the Riemann-solver scalars that
+ * State.set_cparam copies into the /cparam/ common block (state.py:162-182).
+ */
+typedef struct claw2_problem {
+    int32_t rp;                       /* enum claw2_rp                              */
+    int32_t num_eqn;
+    int32_t num_waves;
+    int32_t num_aux;
+    int32_t mx, my;                   /* interior cells                             */
+    int32_t num_ghost;                /* must be CLAW2_NUM_GHOST                    */
+    int32_t order;                    /* method(2): 1 or 2                          */
+    int32_t transverse;               /* method(3): 0,1,2; -1 = dimensional split   */
+    int32_t index_capa;               /* method(6)-1: 0-based aux index, -1 = none  */
+    int32_t use_fwave;                /* solver.fwave                               */
+    int32_t mthlim[CLAW2_MAX_WAVES];  /* solver.limiters per wave family            */
+    int32_t bc_lower[2], bc_upper[2]; /* solver.bc_lower / bc_upper (x, y)          */
+    int32_t aux_bc_lower[2], aux_bc_upper[2];
+    double dx, dy;
+    double params[CLAW2_MAX_PARAMS];  /* acoustics: rho,bulk,cc,zz; euler: gamma,gamma1;
+                                         shallow: grav                              */
+} claw2_problem;
+
+/* Device layout of one ghosted array (see top of file). */
+typedef struct claw2_layout {
+    int64_t ld;        /* row pitch in doubles                                      */
+    int64_t rows;      /* my + 2*num_ghost                                          */
+    int64_t plane;     /* doubles per component plane                               */
+    int64_t q_elems;   /* num_eqn * plane                                           */
+    int64_t aux_elems; /* num_aux * plane                                           */
+} claw2_layout;
+
+/*
+ * Time-step controller kept in device memory.  It restates the loop body of
+ * Solver.evolve_to_time (src/pyclaw/solver.py:632-691): dt clamping to tend,
+ * CFL accept/reject with restore, dt <- min(dt_max, dt*cfl_desired/cfl), and
+ * the status dictionary {cflmax, dtmin, dtmax, numsteps}.  The step kernel's
+ * last block runs that logic on the device, so many steps can be launched (or
+ * replayed from a CUDA graph) without a host round trip per step.
+ */
+typedef struct claw2_control {
+    double t, dt, tstart, tend;
+    double cfl;                 /* CFL number of the last step taken            */
+    double cfl_max, cfl_desired, dt_max;
+    double status_cflmax, status_dtmin, status_dtmax;
+    int64_t numsteps;           /* accepted steps (status['numsteps'])          */
+    int64_t iter;               /* loop iterations including rejected ones      */
+    int64_t max_steps;
+    int64_t rejected;
+    int32_t cur;                /* index (0/1) of the buffer holding the state  */
+    int32_t done;               /* 1 once t >= tend (or one step taken)         */
+    int32_t error;              /* claw2_status of the device loop              */
+    int32_t dt_variable;
+    int32_t take_one_step;
+    uint32_t ticket;            /* block-arrival counter (kept 0 between steps) */
+    int32_t pad_[2];
+} claw2_control;
+
+/* ---- queries --------------------------------------------------------- */
+int claw2_abi_version(void);
+const char* claw2_strerror(int status);
+/* Validates a problem; mirrors the checks the reference performs before it
+ * steps (limiter list length, classic/solver.py:173-176; cparam keys,
+ * state.py:176-180; workspace sizes, step2.f90:66-71). */
+int claw2_validate(const claw2_problem* p);
+int claw2_get_layout(const claw2_problem* p, claw2_layout* out);
+/* Bytes of device scratch (per-block CFL partials) that claw2_step and
+ * claw2_advance need. */
+size_t claw2_scratch_bytes(const claw2_problem* p);
+
+/* ---- device-resident path (device layout, device pointers) ----------- */
+
+/* Fill the ghost cells of q: Solver.apply_q_bcs / qbc_lower / qbc_upper
+ * (src/pyclaw/solver.py:299-434) for extrap/periodic/wall; CUSTOM sides are
+ * left untouched. x first, then y, so corners follow the reference. */
+int claw2_fill_ghosts(const claw2_problem* p, double* q, void* stream);
+/* Same for aux: Solver.apply_aux_bcs / auxbc_lower / auxbc_upper (:438-576). */
+int claw2_fill_aux_ghosts(const claw2_problem* p, double* aux, void* stream);
+
+/* One homogeneous step q_in -> q_out with a given dt: the work of
+ * step2 (src/pyclaw/classic/step2.f90:2-251) when p->transverse >= 0, or of the
+ * two step2ds sweeps (step2ds.f90:2-258, called from classic/solver.py:525-533)
+ * when p->transverse == -1.  q_in's ghost cells must be filled.  Writes the
+ * interior of q_out and, for non-CUSTOM sides, its ghost cells for the next
+ * step.  The CFL number is written to *cfl_dev (device memory).  scratch must
+ * hold claw2_scratch_bytes(p) bytes; its first 64 bytes must be zero on the
+ * first call (the kernel leaves them zero). */
+int claw2_step(const claw2_problem* p, const double* q_in, double* q_out,
+               const double* aux, double dt, void* scratch, double* cfl_dev,
+               void* stream);
+
+/* Launch nsteps controlled steps.  q0/q1 are the two state buffers; ctrl->cur
+ * says which holds the current state.  Each launch reads dt from ctrl, steps
+ * q[cur] -> q[1-cur] and updates ctrl exactly as one iteration of
+ * Solver.evolve_to_time (solver.py:632-691) does.  Launches after ctrl->done
+ * become no-ops.  Nothing is synchronised; read ctrl back to see progress. */
+int claw2_advance(const claw2_problem* p, double* q0, double* q1,
+                  const double* aux, claw2_control* ctrl, void* scratch,
+                  int nsteps, void* stream);
+
+/* Host-side initialisation of a controller for evolve_to_time(solution, tend)
+ * (solver.py:600-641): status reset, fixed-dt step count, first clamp. */
+int claw2_control_init(claw2_control* c, double t, double dt, double tend,
+                       double cfl_max, double cfl_desired, double dt_max,
+                       int dt_variable, int take_one_step, int64_t max_steps,
+                       double prev_cfl);
+
+/* Layout conversion between the reference layout and the device layout, on
+ * the device (device pointers to both). */
+int claw2_ref_to_device(const claw2_problem* p, int ncomp, const double* ref,
+                        double* dev, void* stream);
+int claw2_device_to_ref(const claw2_problem* p, int ncomp, const double* dev,
+                        double* ref, void* stream);
+
+/* ---- host-buffer session (reference layout, host pointers) ----------- */
+/* A session owns device buffers for one problem so that callers holding host
+ * arrays (the f2py calling convention of step2) can step without managing
+ * device memory. */
+typedef struct claw2_session claw2_session;
+int claw2_session_create(const claw2_problem* p, claw2_session** out);
+int claw2_session_destroy(claw2_session* s);
+/* Exact f2py contract of step2/step2ds (classic/solver.py:525-539): qold and
+ * qnew are host arrays in reference layout with ghost cells already filled by
+ * the caller; on return qnew holds the updated array and *cfl the CFL number.
+ * aux may be NULL when num_aux == 0. */
+int claw2_session_step2(claw2_session* s, const double* qold, double* qnew,
+                        const double* aux, double dt, double* cfl);
+/* Controller.run-style evolve from host data: q (reference layout interior,
+ * shape (num_eqn, mx, my) Fortran order) is uploaded, the solution is advanced
+ * from *t to tend with on-device dt control, and q is downloaded again.
+ * *t and *dt are updated; status receives {cflmax, dtmin, dtmax, numsteps,
+ * rejected} as doubles (5 entries, may be NULL). */
+int claw2_session_evolve(claw2_session* s, double* q, const double* aux,
+                         double* t, double* dt, double tend, double cfl_max,
+                         double cfl_desired, double dt_max, int64_t max_steps,
+                         double* status);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CLAW2_H */

@@ -1,0 +1,69 @@
+"""Pin the CPU oracle to the reference's own known-answer tests.
+
+Each case reruns a reference application (restated in tests/kat_setups.py)
+through the oracle and applies the reference test's own comparison:
+  apps/euler_2d/test_euler2d_shockbubble.py:15-19       abstol 1e-12 (2-norm)
+  apps/acoustics_2d_homogeneous/test_2d_acoustics.py:115-116   reltol 1e-3
+  apps/acoustics_2d_variable/test_acoustics_2d_variable.py:111-115  max-abs 0.1
+  apps/acoustics_2d_variable/test_acoustics_2d_variable_io.py:146-182 reltol 1e-4
+"""
+import os
+
+import numpy as np
+
+import kat_setups as K
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def test_shockbubble_split_euler5_matches_reference(orc):
+    p, q, aux, run, bcs, src = K.shockbubble_setup()
+    r = orc.Run(p, q, aux, bc_callbacks=bcs, step_source=src, **run)
+    frames = r.run(0.2, num_output_times=1)
+    gold = np.load(os.path.join(GOLD, "shockbubble_density.npz"))["density"]
+    err = np.linalg.norm(gold - frames[-1][0])
+    assert K.check_diff(0, err, abstol=1e-12) is None, err
+
+
+def test_acoustics_homogeneous_split_matches_reference(orc):
+    p, q, aux, run = K.acoustics_homogeneous_setup()
+    r = orc.Run(p, q, aux, **run)
+    frames = r.run(0.12, num_output_times=10)
+    gold = np.load(os.path.join(GOLD, "acoustics_pressure.npz"))["pressure"]
+    assert K.check_diff(gold, frames[-1][0], reltol=1e-3) is None
+
+
+def test_acoustics_variable_unsplit_matches_reference(orc):
+    p, q, aux, run = K.acoustics_variable_setup()
+    r = orc.Run(p, q, aux, **run)
+    frames = r.run(0.6, num_output_times=20)
+    gold = np.load(os.path.join(GOLD, "vc_acoustics_pressure.npz"))["pressure"]
+    err = np.max(np.abs(gold - frames[20][0]))
+    assert K.check_diff(0, err, abstol=1e-1) is None
+    # far tighter than the reference's own bound: the restated solver agrees
+    # with the 18-digit golden file to round-off
+    assert err < 1e-13, err
+    io = np.load(os.path.join(GOLD, "vc_acoustics_io.npz"))
+    assert K.check_diff(io["q20"], frames[20], reltol=1e-4) is None
+    assert K.check_diff(io["aux0"], aux, reltol=1e-4) is None
+    assert float(io["t20"]) == 0.6 and abs(r.t - 0.6) < 1e-14
+
+
+def test_omp_gather_form_is_bit_identical(orc):
+    """The multi-threaded baseline build reproduces the serial interior exactly."""
+    for setup, tr in ((K.acoustics_variable_setup, 2), (K.acoustics_variable_setup, -1)):
+        p, q, aux, run = setup(mx=37, my=29)
+        p.transverse = tr
+        qbc = orc.new_qbc(p, q)
+        auxbc = orc.new_qbc(p, aux, p.num_aux)
+        orc.fill_aux_ghosts(p, auxbc)
+        a = qbc.copy(order="F")
+        b = qbc.copy(order="F")
+        for _ in range(5):
+            orc.fill_ghosts(p, a)
+            orc.fill_ghosts(p, b)
+            ca = orc.step_hyperbolic(p, a, auxbc, 0.004)
+            cb = orc.step_hyperbolic(p, b, auxbc, 0.004, omp=True)
+            assert ca == cb
+            g = p.num_ghost
+            assert np.array_equal(a[:, g:-g, g:-g], b[:, g:-g, g:-g])
