@@ -1,0 +1,472 @@
+"""Benchmark: FP64 cell-updates/s of the 2D wave-propagation step on B200.
+
+Workload (one "step" = one controlled time step of the whole grid):
+  2D Euler shock-bubble, 1280x320 cells on [0,2]x[0,0.5], gamma=1.4, q=(rho,
+  rhou,rhov,E); Mach-2 planar shock at x=0.2 moving +x into still air (rho=1,
+  p=1), post-shock state from the Rankine-Hugoniot relations (p=4.5, rho=8/3,
+  u=2*sqrt(1.4)*(1-3/8)); circular bubble rho=0.1, p=1, centre (0.5,0.25),
+  radius 0.2 (cell-centre indicator); Roe solver with Harten-Hyman entropy fix,
+  MC limiter, unsplit with transverse_waves=2, extrapolation BCs in x, walls in
+  y, cfl_desired 0.9 / cfl_max 1.0.  Synthetic data of the reference's shape.
+
+Usage:
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One JSON line is printed by rank 0.  ``value`` is whole-job cell-updates/s
+with the state resident in HBM (device-timed, L2 flushed between timed steps);
+``e2e`` is the same metric through the host-buffer C ABI
+(claw2_session_evolve: host state in, host state out, each call advancing
+the solution by a fixed simulated interval).  With N > 1 the ranks run
+independent replicas of the workload (the single-grid step has no exchange on
+one GPU; see the design notes) and the value is the sum over ranks.
+"""
+import argparse
+import ctypes
+import json
+import math
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+GAMMA = 1.4
+
+
+# ---------------------------------------------------------------------------
+# workload definitions (shared with the tests)
+# ---------------------------------------------------------------------------
+def _centers(lower, upper, n):
+    delta = (upper - lower) / float(n)
+    c = np.empty(n)
+    for i in range(n):
+        c[i] = lower + (i + 0.5) * delta
+    return c, delta
+
+
+def shockbubble_config(mx=1280, my=320, walls=False):
+    """Returns (problem, q0, aux0, run_kwargs, tfinal) for the shock-bubble workload."""
+    from pyclaw_b200 import _abi
+    x, dx = _centers(0.0, 2.0, mx)
+    y, dy = _centers(0.0, 0.5, my)
+    X, Y = np.meshgrid(x, y, indexing='ij')
+    gamma1 = GAMMA - 1.0
+    # Rankine-Hugoniot post-shock state for a Mach-2 shock into rho=1, p=1, u=0
+    M = 2.0
+    p2 = 1.0 + 2.0 * GAMMA / (GAMMA + 1.0) * (M * M - 1.0)
+    rho2 = (GAMMA + 1.0) * M * M / ((GAMMA - 1.0) * M * M + 2.0)
+    u2 = M * np.sqrt(GAMMA) * (1.0 - 1.0 / rho2)
+    behind = X < 0.2
+    bubble = np.sqrt((X - 0.5) ** 2 + (Y - 0.25) ** 2) <= 0.2
+    rho = np.where(behind, rho2, np.where(bubble, 0.1, 1.0))
+    u = np.where(behind, u2, 0.0)
+    p = np.where(behind, p2, 1.0)
+    q = np.empty((4, mx, my), order='F')
+    q[0] = rho
+    q[1] = rho * u
+    q[2] = 0.0
+    q[3] = p / gamma1 + 0.5 * rho * u * u
+    bcx = _abi.BC_WALL if walls else _abi.BC_EXTRAP
+    prob = _abi.make_problem(rp=_abi.RP_EULER_4WAVE, num_eqn=4, num_waves=4, num_aux=0, mx=mx, my=my,
+                             dx=dx, dy=dy, order=2, transverse=2, mthlim=[4],
+                             bc_lower=(bcx, _abi.BC_WALL), bc_upper=(bcx, _abi.BC_WALL),
+                             params=(GAMMA, gamma1))
+    smax = abs(u2) + np.sqrt(GAMMA * p2 / rho2)
+    run = dict(cfl_max=1.0, cfl_desired=0.9, dt_initial=0.9 * min(dx, dy) / smax)
+    return prob, q, None, run, 0.6
+
+
+def acoustics_config(n=256):
+    """256^2 constant-coefficient acoustics on [-1,1]^2, rho=1, K=4, walls,
+    p = exp(-((r-0.25)/0.05)^2), unsplit trans=2, MC, cfl 0.9, t=0.6."""
+    from pyclaw_b200 import _abi
+    x, dx = _centers(-1.0, 1.0, n)
+    y, dy = _centers(-1.0, 1.0, n)
+    X, Y = np.meshgrid(x, y, indexing='ij')
+    rho, bulk = 1.0, 4.0
+    cc = np.sqrt(bulk / rho)
+    zz = rho * cc
+    r = np.sqrt(X ** 2 + Y ** 2)
+    q = np.empty((3, n, n), order='F')
+    q[0] = np.exp(-((r - 0.25) / 0.05) ** 2)
+    q[1] = 0.0
+    q[2] = 0.0
+    prob = _abi.make_problem(rp=_abi.RP_ACOUSTICS, num_eqn=3, num_waves=2, num_aux=0, mx=n, my=n,
+                             dx=dx, dy=dy, order=2, transverse=2, mthlim=[4],
+                             bc_lower=(_abi.BC_WALL, _abi.BC_WALL), bc_upper=(_abi.BC_WALL, _abi.BC_WALL),
+                             params=(rho, bulk, cc, zz))
+    run = dict(cfl_max=1.0, cfl_desired=0.9, dt_initial=0.9 * dx / cc)
+    return prob, q, None, run, 0.6
+
+
+def make_solver(pc, prob, run):
+    """A ClawSolver2D configured like `prob` (Euler shock-bubble settings)."""
+    solver = pc.ClawSolver2D(pc.riemann.rp2_euler_4wave)
+    solver.dimensional_split = False
+    solver.transverse_waves = int(prob.transverse)
+    solver.limiters = [int(prob.mthlim[w]) for w in range(prob.num_waves)]
+    solver.bc_lower = [int(prob.bc_lower[0]), int(prob.bc_lower[1])]
+    solver.bc_upper = [int(prob.bc_upper[0]), int(prob.bc_upper[1])]
+    solver.cfl_max = run['cfl_max']
+    solver.cfl_desired = run['cfl_desired']
+    solver.dt_initial = run['dt_initial']
+    return solver
+
+
+# ---------------------------------------------------------------------------
+# helpers
+# ---------------------------------------------------------------------------
+def _peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler(object):
+    """nvidia-smi clock/throttle sampling during the timed region."""
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", "clocks_bench_%d.csv" % gpu_index)
+
+    def start(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), "--query-gpu=" + self.QUERY,
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.f.close()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for ln in f:
+                parts = [s.strip() for s in ln.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    mx = float(parts[2])
+                except ValueError:
+                    continue
+                for n, v in zip(names, parts[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def _dist_init():
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if torch.cuda.is_available():
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+    elif torch.cuda.is_available():
+        torch.cuda.set_device(local)
+    return world, rank, local
+
+
+def _barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def _max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda" if torch.cuda.is_available() else "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def _sum_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda" if torch.cuda.is_available() else "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------------------
+# CPU arms (oracle = C restatement of the reference Fortran step)
+# ---------------------------------------------------------------------------
+def cpu_rate(prob, q, run, omp, max_seconds=15.0, max_steps=None):
+    """Time whole-grid oracle steps (BC fill + step + dt control) on the host;
+    returns (cell-updates/s, steps timed, threads, seconds)."""
+    from oracle import oracle as O
+    lib = O.load(omp)
+    qbc = O.new_qbc(prob, q)
+    ctrl = O.control_init(0.0, run['dt_initial'], 1e9, run['cfl_max'], run['cfl_desired'], lib=O.load())
+    threads = lib.orc_num_threads() if omp else 1
+    cells = prob.mx * prob.my
+    steps = 0
+    accepted0 = ctrl.numsteps
+    t0 = time.perf_counter()
+    while True:
+        ctrl.done = 0
+        ctrl.error = 0
+        ctrl.max_steps = ctrl.iter + 1
+        rc = O.evolve(prob, qbc, None, ctrl, omp=omp)
+        if rc not in (0, 5):
+            raise RuntimeError("oracle evolve failed: %d" % rc)
+        steps += 1
+        el = time.perf_counter() - t0
+        if el >= max_seconds or (max_steps is not None and steps >= max_steps):
+            break
+    accepted = ctrl.numsteps - accepted0
+    return accepted * cells / el, steps, threads, el
+
+
+def run_reference_arm(args, world, rank):
+    """--impl reference: the oracle (OpenMP gather form, all host threads)."""
+    if rank != 0:
+        return
+    prob, q, aux, run, tfinal = shockbubble_config()
+    from oracle import oracle as O
+    lib = O.load(True)
+    qbc = O.new_qbc(prob, q)
+    ctrl = O.control_init(0.0, run['dt_initial'], 1e9, run['cfl_max'], run['cfl_desired'], lib=O.load())
+    threads = lib.orc_num_threads()
+    cells = prob.mx * prob.my
+
+    def one_step():
+        ctrl.done = 0
+        ctrl.error = 0
+        ctrl.max_steps = ctrl.iter + 1
+        rc = O.evolve(prob, qbc, None, ctrl, omp=True)
+        if rc not in (0, 5):
+            raise RuntimeError("oracle evolve failed: %d" % rc)
+
+    for _ in range(args.warmup):
+        one_step()
+    a0 = ctrl.numsteps
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        one_step()
+    el = time.perf_counter() - t0
+    acc = ctrl.numsteps - a0
+    value = acc * cells / el
+    line = {
+        "impl": "reference", "metric": "cell_updates_per_s", "value": value, "unit": "cell-updates/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": el / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "euler_shockbubble_1280x320", "mx": prob.mx, "my": prob.my,
+                   "solver": "euler_roe_efix_4wave", "limiter": "MC", "transverse_waves": 2},
+        "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": threads, "kind": "port",
+                         "sample": "%d whole-grid steps (BC fill + step + dt control) of the 1280x320 "
+                                   "shock bubble, oracle OpenMP gather form, %d threads" % (args.steps, threads)},
+        "e2e": {"value": value, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+def run_ours(args, world, rank, local):
+    import torch
+    import pyclaw_b200 as pc
+    from pyclaw_b200 import _abi, _lib
+    from pyclaw_b200.device import DeviceState
+
+    lib = _lib.load()
+    prob, q, aux, run, tfinal = shockbubble_config()
+    cells = prob.mx * prob.my
+    dev = DeviceState(prob, torch.device("cuda", local))
+    dev.upload_q(q)
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    c = _abi.Control()
+    _lib.check(lib.claw2_control_init(ctypes.byref(c), 0.0, run['dt_initial'], 1e9, run['cfl_max'],
+                                      run['cfl_desired'], 1e99, 1, 0, 1 << 40, run['cfl_desired']),
+               "claw2_control_init")
+    host = _abi.Control.from_address(dev.ctrl_host.data_ptr())
+    ctypes.memmove(ctypes.addressof(host), ctypes.addressof(c), ctypes.sizeof(c))
+    dev.ctrl.copy_(dev.ctrl_host)
+    flush = torch.empty(256 * 1024 * 1024 // 8, dtype=torch.float64, device="cuda")   # 256 MB > L2
+
+    def advance(n):
+        _lib.check(lib.claw2_advance(ctypes.byref(prob), dev.ptr(dev.q[0]), dev.ptr(dev.q[1]), dev.ptr(dev.aux),
+                                     dev.ptr(dev.ctrl), dev.ptr(dev.scratch), int(n), dev.stream), "claw2_advance")
+
+    for _ in range(max(3, args.warmup)):
+        flush.fill_(1.0)
+        advance(1)
+    torch.cuda.synchronize()
+    dev.ctrl_host.copy_(dev.ctrl)
+    n0 = host.numsteps
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    clocks = ClockSampler(torch.cuda.current_device()) if rank == 0 or world > 1 else None
+    if clocks:
+        clocks.start()
+    _barrier(world)
+    torch.cuda.synchronize()
+    w0 = time.perf_counter()
+    for k in range(args.steps):
+        flush.fill_(float(k))                 # evict the state from L2 (not timed)
+        ev[k][0].record(stream)
+        advance(1)
+        ev[k][1].record(stream)
+    torch.cuda.synchronize()
+    _barrier(world)
+    wall = time.perf_counter() - w0
+    clk = clocks.stop() if clocks else None
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    t_dev = sum(step_ms) / 1e3
+    dev.ctrl_host.copy_(dev.ctrl)
+    torch.cuda.synchronize()
+    accepted = host.numsteps - n0
+    if host.error:
+        raise RuntimeError("device loop error %d" % host.error)
+    t_max = _max_over_ranks(t_dev, world)
+    total_updates = _sum_over_ranks(float(accepted * cells), world)
+    value = total_updates / t_max
+
+    # ---- roofline of the step kernel ----------------------------------------
+    peak, peak_kind = _peaks()
+    alg_bytes = 8 * (2 * prob.num_eqn + prob.num_aux) * cells   # per launch (one step)
+    avg_kernel_s = t_dev / args.steps
+    achieved = alg_bytes / avg_kernel_s / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "step_kernel_traffic.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            tj = json.load(f)
+        traffic = tj.get("dram_bytes_per_launch_scaled")
+
+    # ---- e2e through the host-buffer C ABI (claw2_session_evolve) ----------
+    e2e = None
+    if rank == 0 or world > 1:
+        e2e = _e2e(lib, prob, q, run, args)
+    e2e_val = _sum_over_ranks(e2e["value"], world) if e2e else None
+
+    # ---- CPU baseline (oracle, all host threads; bounded sample) ---------------
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        rate, n, thr, el = cpu_rate(prob, q, run, omp=True, max_seconds=12.0)
+        rate1, n1, _, el1 = cpu_rate(prob, q, run, omp=False, max_seconds=8.0)
+        cpu = {"value": rate, "unit": "cell-updates/s", "cores": thr, "kind": "port",
+               "sample": "%d whole-grid steps (%.1f s) of the 1280x320 shock bubble through the oracle's "
+                         "OpenMP gather form on %d threads; serial oracle: %.4g cell-updates/s over %d steps"
+                         % (n, el, thr, rate1, n1)}
+
+    if rank == 0:
+        line = {
+            "metric": "cell_updates_per_s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": "euler_shockbubble_1280x320", "mx": prob.mx, "my": prob.my,
+                       "solver": "euler_roe_efix_4wave", "limiter": "MC", "transverse_waves": 2,
+                       "parallelism": "replicas" if world > 1 else "single",
+                       "l2": "flushed (256 MB write) before every timed step",
+                       "accepted_steps": int(accepted)},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "peak_source": peak_kind,
+                         "algorithmic_bytes_per_launch": alg_bytes},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_val, "unit": "cell-updates/s",
+                    "h2d_bytes_per_step": e2e["h2d"], "d2h_bytes_per_step": e2e["d2h"],
+                    "steps_per_call": e2e["steps"], "calls": e2e["calls"]} if e2e else None,
+            "gpu_launches": int(args.steps),
+            "clocks": clk,
+            "wall_s": wall,
+        }
+        print(json.dumps(line), flush=True)
+
+
+def _e2e(lib, prob, q, run, args):
+    """claw2_session_evolve from pinned host buffers: each call uploads the
+    state, advances it by a fixed simulated interval with on-device dt
+    control, and downloads it again."""
+    import torch
+    s = ctypes.c_void_p()
+    from pyclaw_b200 import _lib
+    _lib.check(lib.claw2_session_create(ctypes.byref(prob), ctypes.byref(s)), "claw2_session_create")
+    try:
+        host = torch.from_numpy(np.asfortranarray(q).ravel(order='K')).clone().pin_memory()
+        hq = host.numpy()
+        t = ctypes.c_double(0.0)
+        dt = ctypes.c_double(run['dt_initial'])
+        status = (ctypes.c_double * 5)()
+        interval = 40 * run['dt_initial']
+        def call():
+            return lib.claw2_session_evolve(s, hq.ctypes.data, None, ctypes.byref(t), ctypes.byref(dt),
+                                            t.value + interval, run['cfl_max'], run['cfl_desired'], 1e99,
+                                            100000, status)
+        _lib.check(call(), "claw2_session_evolve")     # warm-up
+        calls = max(2, min(args.steps, 8))
+        steps = 0
+        t0 = time.perf_counter()
+        for _ in range(calls):
+            _lib.check(call(), "claw2_session_evolve")
+            steps += int(status[3])
+        el = time.perf_counter() - t0
+        nbytes = 8 * prob.num_eqn * prob.mx * prob.my
+        return {"value": steps * prob.mx * prob.my / el, "h2d": nbytes, "d2h": nbytes,
+                "steps": steps / calls, "calls": calls}
+    finally:
+        lib.claw2_session_destroy(s)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    world, rank, local = _dist_init()
+    try:
+        if args.impl == "reference":
+            run_reference_arm(args, world, rank)
+        else:
+            run_ours(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

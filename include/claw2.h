@@ -35,6 +35,10 @@
 #include <stddef.h>
 #include <stdint.h>
 
+#ifndef CLAW2_EXPORT
+#define CLAW2_EXPORT
+#endif
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -132,30 +136,30 @@ typedef struct claw2_control {
     int32_t error;              /* claw2_status of the device loop              */
     int32_t dt_variable;
     int32_t take_one_step;
-    uint32_t ticket;            /* block-arrival counter (kept 0 between steps) */
+    uint32_t reserved_;         /* keep 0 (the block-arrival counter lives in scratch) */
     int32_t pad_[2];
 } claw2_control;
 
 /* ---- queries --------------------------------------------------------- */
-int claw2_abi_version(void);
-const char* claw2_strerror(int status);
+CLAW2_EXPORT int claw2_abi_version(void);
+CLAW2_EXPORT const char* claw2_strerror(int status);
 /* Validates a problem; mirrors the checks the reference performs before it
  * steps (limiter list length, classic/solver.py:173-176; cparam keys,
  * state.py:176-180; workspace sizes, step2.f90:66-71). */
-int claw2_validate(const claw2_problem* p);
-int claw2_get_layout(const claw2_problem* p, claw2_layout* out);
+CLAW2_EXPORT int claw2_validate(const claw2_problem* p);
+CLAW2_EXPORT int claw2_get_layout(const claw2_problem* p, claw2_layout* out);
 /* Bytes of device scratch (per-block CFL partials) that claw2_step and
  * claw2_advance need. */
-size_t claw2_scratch_bytes(const claw2_problem* p);
+CLAW2_EXPORT size_t claw2_scratch_bytes(const claw2_problem* p);
 
 /* ---- device-resident path (device layout, device pointers) ----------- */
 
 /* Fill the ghost cells of q: Solver.apply_q_bcs / qbc_lower / qbc_upper
  * (src/pyclaw/solver.py:299-434) for extrap/periodic/wall; CUSTOM sides are
  * left untouched. x first, then y, so corners follow the reference. */
-int claw2_fill_ghosts(const claw2_problem* p, double* q, void* stream);
+CLAW2_EXPORT int claw2_fill_ghosts(const claw2_problem* p, double* q, void* stream);
 /* Same for aux: Solver.apply_aux_bcs / auxbc_lower / auxbc_upper (:438-576). */
-int claw2_fill_aux_ghosts(const claw2_problem* p, double* aux, void* stream);
+CLAW2_EXPORT int claw2_fill_aux_ghosts(const claw2_problem* p, double* aux, void* stream);
 
 /* One homogeneous step q_in -> q_out with a given dt: the work of
  * step2 (src/pyclaw/classic/step2.f90:2-251) when p->transverse >= 0, or of the
@@ -165,7 +169,7 @@ int claw2_fill_aux_ghosts(const claw2_problem* p, double* aux, void* stream);
  * step.  The CFL number is written to *cfl_dev (device memory).  scratch must
  * hold claw2_scratch_bytes(p) bytes; its first 64 bytes must be zero on the
  * first call (the kernel leaves them zero). */
-int claw2_step(const claw2_problem* p, const double* q_in, double* q_out,
+CLAW2_EXPORT int claw2_step(const claw2_problem* p, const double* q_in, double* q_out,
                const double* aux, double dt, void* scratch, double* cfl_dev,
                void* stream);
 
@@ -174,22 +178,22 @@ int claw2_step(const claw2_problem* p, const double* q_in, double* q_out,
  * q[cur] -> q[1-cur] and updates ctrl exactly as one iteration of
  * Solver.evolve_to_time (solver.py:632-691) does.  Launches after ctrl->done
  * become no-ops.  Nothing is synchronised; read ctrl back to see progress. */
-int claw2_advance(const claw2_problem* p, double* q0, double* q1,
+CLAW2_EXPORT int claw2_advance(const claw2_problem* p, double* q0, double* q1,
                   const double* aux, claw2_control* ctrl, void* scratch,
                   int nsteps, void* stream);
 
 /* Host-side initialisation of a controller for evolve_to_time(solution, tend)
  * (solver.py:600-641): status reset, fixed-dt step count, first clamp. */
-int claw2_control_init(claw2_control* c, double t, double dt, double tend,
+CLAW2_EXPORT int claw2_control_init(claw2_control* c, double t, double dt, double tend,
                        double cfl_max, double cfl_desired, double dt_max,
                        int dt_variable, int take_one_step, int64_t max_steps,
                        double prev_cfl);
 
 /* Layout conversion between the reference layout and the device layout, on
  * the device (device pointers to both). */
-int claw2_ref_to_device(const claw2_problem* p, int ncomp, const double* ref,
+CLAW2_EXPORT int claw2_ref_to_device(const claw2_problem* p, int ncomp, const double* ref,
                         double* dev, void* stream);
-int claw2_device_to_ref(const claw2_problem* p, int ncomp, const double* dev,
+CLAW2_EXPORT int claw2_device_to_ref(const claw2_problem* p, int ncomp, const double* dev,
                         double* ref, void* stream);
 
 /* ---- host-buffer session (reference layout, host pointers) ----------- */
@@ -197,20 +201,20 @@ int claw2_device_to_ref(const claw2_problem* p, int ncomp, const double* dev,
  * arrays (the f2py calling convention of step2) can step without managing
  * device memory. */
 typedef struct claw2_session claw2_session;
-int claw2_session_create(const claw2_problem* p, claw2_session** out);
-int claw2_session_destroy(claw2_session* s);
+CLAW2_EXPORT int claw2_session_create(const claw2_problem* p, claw2_session** out);
+CLAW2_EXPORT int claw2_session_destroy(claw2_session* s);
 /* Exact f2py contract of step2/step2ds (classic/solver.py:525-539): qold and
  * qnew are host arrays in reference layout with ghost cells already filled by
  * the caller; on return qnew holds the updated array and *cfl the CFL number.
  * aux may be NULL when num_aux == 0. */
-int claw2_session_step2(claw2_session* s, const double* qold, double* qnew,
+CLAW2_EXPORT int claw2_session_step2(claw2_session* s, const double* qold, double* qnew,
                         const double* aux, double dt, double* cfl);
 /* Controller.run-style evolve from host data: q (reference layout interior,
  * shape (num_eqn, mx, my) Fortran order) is uploaded, the solution is advanced
  * from *t to tend with on-device dt control, and q is downloaded again.
  * *t and *dt are updated; status receives {cflmax, dtmin, dtmax, numsteps,
  * rejected} as doubles (5 entries, may be NULL). */
-int claw2_session_evolve(claw2_session* s, double* q, const double* aux,
+CLAW2_EXPORT int claw2_session_evolve(claw2_session* s, double* q, const double* aux,
                          double* t, double* dt, double tend, double cfl_max,
                          double cfl_desired, double dt_max, int64_t max_steps,
                          double* status);

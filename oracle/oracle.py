@@ -152,9 +152,10 @@ class Run:
 
     def __init__(self, p, q, aux=None, *, cfl_max=1.0, cfl_desired=0.9, dt_initial=0.1,
                  dt_max=1e99, dt_variable=True, max_steps=10000, bc_callbacks=None,
-                 step_source=None, source_split=1, lib=None):
+                 step_source=None, source_split=1, lib=None, omp=False):
         self.p = p
-        self.lib = lib or load()
+        self.omp = omp
+        self.lib = lib or load(omp)
         g = p.num_ghost
         self.qbc = new_qbc(p, q)
         self.q = self.qbc[:, g:-g, g:-g]
@@ -213,7 +214,7 @@ class Run:
     def step(self):
         """ClawSolver.step (classic/solver.py:100-151); returns True on success."""
         self.apply_q_bcs()
-        self.cfl = step_hyperbolic(self.p, self.qbc, self.auxbc, self.dt, lib=self.lib)
+        self.cfl = step_hyperbolic(self.p, self.qbc, self.auxbc, self.dt, lib=self.lib, omp=self.omp)
         g = self.p.num_ghost
         self.q = self.qbc[:, g:-g, g:-g]
         if self.cfl >= self.cfl_max:

@@ -97,7 +97,7 @@ class Control(ctypes.Structure):
         ("error", ctypes.c_int32),
         ("dt_variable", ctypes.c_int32),
         ("take_one_step", ctypes.c_int32),
-        ("ticket", ctypes.c_uint32),
+        ("reserved_", ctypes.c_uint32),
         ("pad_", ctypes.c_int32 * 2),
     ]
 

@@ -1,0 +1,578 @@
+// claw2_capi.cu -- CUDA kernels and the extern "C" ABI declared in include/claw2.h.
+//
+// Built for sm_100a with --fmad=false (no FMA contraction, so the step
+// reproduces the reference's operation-by-operation rounding).
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdint>
+#include <cstdlib>
+#include <cstring>
+#include <new>
+
+#define CLAW2_EXPORT __attribute__((visibility("default")))
+#include "../../include/claw2.h"
+#include "claw2_kernels.cuh"
+
+namespace claw2 {
+
+// ---------------------------------------------------------------------------
+// device execution context for step_tile
+// ---------------------------------------------------------------------------
+struct DevCtx {
+    double* sm;
+    __device__ __forceinline__ int tid() const { return threadIdx.x; }
+    __device__ __forceinline__ int bx() const { return blockIdx.x; }
+    __device__ __forceinline__ int by() const { return blockIdx.y; }
+    __device__ __forceinline__ int nbx() const { return gridDim.x; }
+    __device__ __forceinline__ int nby() const { return gridDim.y; }
+    __device__ __forceinline__ void sync() const { __syncthreads(); }
+    __device__ __forceinline__ void fence() const { __threadfence(); }
+    __device__ __forceinline__ unsigned atomic_inc(unsigned* p) const { return atomicAdd(p, 1u); }
+    __device__ __forceinline__ double load_volatile(const double* p) const { return *(volatile const double*)p; }
+    __device__ __forceinline__ double nan() const { return __longlong_as_double(0x7ff8000000000000ULL); }
+    __device__ __forceinline__ double* smem() const { return sm; }
+};
+
+template <class RP, int TX, int TY, int NT, bool SPLIT>
+__global__ void __launch_bounds__(NT) step_kernel(StepArgs a)
+{
+    extern __shared__ double smem_dyn[];
+    DevCtx ctx{smem_dyn};
+    step_tile<RP, TX, TY, NT, SPLIT>(a, ctx);
+}
+
+// Tile shapes: a line of a chunk has 32 interface slots, so TX+3, TY+3 <= 32.
+constexpr int UTX = 29, UTY = 29, UNT = 256;   // unsplit
+constexpr int STX = 28, STY = 28, SNT = 256;   // dimensional splitting
+
+// ---------------------------------------------------------------------------
+// ghost fill (device layout): Solver.apply_q_bcs, x sides then y sides
+// ---------------------------------------------------------------------------
+struct FillArgs {
+    double* q;
+    long long ld, plane;
+    int mx, my, ncomp;
+    int bl, bu;        // this axis' lower/upper BC
+    int negate;        // 0-based component negated at walls (-1 none)
+};
+
+// axis 0 fills ghost columns over all rows (incl. ghost rows); axis 1 fills ghost
+// rows over all columns.  One thread per (component, position along the other
+// axis, ghost layer, side).
+template <int AXIS>
+__device__ __forceinline__ void fill_body(const FillArgs& f)
+{
+    const int other = (AXIS == 0 ? f.my : f.mx) + 2 * CLAW2_NUM_GHOST;
+    const int n = AXIS == 0 ? f.mx : f.my;
+    const long long total = (long long)f.ncomp * other * 2 * CLAW2_NUM_GHOST;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+        const int o = (int)(t % other) - CLAW2_NUM_GHOST;
+        long long r = t / other;
+        const int g = (int)(r % CLAW2_NUM_GHOST);
+        r /= CLAW2_NUM_GHOST;
+        const int side = (int)(r % 2);
+        const int m = (int)(r / 2);
+        const int bc = side == 0 ? f.bl : f.bu;
+        int dst, src;
+        if (side == 0) {
+            dst = -1 - g;
+            if (bc == CLAW2_BC_EXTRAP) src = 0;
+            else if (bc == CLAW2_BC_PERIODIC) src = n - 1 - g;
+            else if (bc == CLAW2_BC_WALL) src = g;
+            else continue;
+        } else {
+            dst = n + g;
+            if (bc == CLAW2_BC_EXTRAP) src = n - 1;
+            else if (bc == CLAW2_BC_PERIODIC) src = g;
+            else if (bc == CLAW2_BC_WALL) src = n - 1 - g;
+            else continue;
+        }
+        auto off = [&](int along) {
+            const int i = AXIS == 0 ? along : o, j = AXIS == 0 ? o : along;
+            return (long long)m * f.plane + (long long)(j + CLAW2_NUM_GHOST) * f.ld + (i + CLAW2_NUM_GHOST);
+        };
+        double v = f.q[off(src)];
+        if (bc == CLAW2_BC_WALL && m == f.negate) v = -v;
+        f.q[off(dst)] = v;
+    }
+}
+
+template <int AXIS>
+__global__ void fill_kernel(FillArgs f)
+{
+    fill_body<AXIS>(f);
+}
+
+// Fill the ghost cells of q[ctrl->cur] (used after controlled steps when the
+// step kernel cannot write ghost images itself).
+template <int AXIS>
+__global__ void fill_kernel_ctrl(FillArgs f, double* q0, double* q1, const claw2_control* c)
+{
+    f.q = c->cur ? q1 : q0;
+    fill_body<AXIS>(f);
+}
+
+// ---------------------------------------------------------------------------
+// layout conversion: reference (m fastest, Fortran) <-> device (planes)
+// ---------------------------------------------------------------------------
+__global__ void ref_to_dev_kernel(const double* ref, double* dev, int nc, int nx, int ny, long long ld,
+                                  long long plane, int ghosts_in_ref)
+{
+    const long long total = (long long)nc * nx * ny;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+        const int m = (int)(t % nc);
+        const long long r = t / nc;
+        const int i = (int)(r % nx), j = (int)(r / nx);
+        const int off = ghosts_in_ref ? 0 : CLAW2_NUM_GHOST;
+        dev[(long long)m * plane + (long long)(j + off) * ld + (i + off)] = ref[t];
+    }
+}
+
+__global__ void dev_to_ref_kernel(const double* dev, double* ref, int nc, int nx, int ny, long long ld,
+                                  long long plane, int ghosts_in_ref)
+{
+    const long long total = (long long)nc * nx * ny;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+        const int m = (int)(t % nc);
+        const long long r = t / nc;
+        const int i = (int)(r % nx), j = (int)(r / nx);
+        const int off = ghosts_in_ref ? 0 : CLAW2_NUM_GHOST;
+        ref[t] = dev[(long long)m * plane + (long long)(j + off) * ld + (i + off)];
+    }
+}
+
+}  // namespace claw2
+
+using namespace claw2;
+
+// ===========================================================================
+// host helpers
+// ===========================================================================
+namespace {
+
+inline cudaStream_t S(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+int solver_shape(int rp, int* meqn, int* mw, int* maux)
+{
+    switch (rp) {
+    case CLAW2_RP_ACOUSTICS: *meqn = 3; *mw = 2; *maux = 0; return 0;
+    case CLAW2_RP_VC_ACOUSTICS: *meqn = 3; *mw = 2; *maux = 2; return 0;
+    case CLAW2_RP_EULER_4WAVE: *meqn = 4; *mw = 4; *maux = 0; return 0;
+    case CLAW2_RP_EULER_5WAVE: *meqn = 5; *mw = 5; *maux = 0; return 0;
+    case CLAW2_RP_SHALLOW_ROE: *meqn = 3; *mw = 3; *maux = 0; return 0;
+    default: return -1;
+    }
+}
+
+bool periodic_ok(int bl, int bu) { return (bl == CLAW2_BC_PERIODIC) == (bu == CLAW2_BC_PERIODIC); }
+
+bool fused_ghosts(const claw2_problem* p)
+{
+    for (int d = 0; d < 2; d++) {
+        if (p->bc_lower[d] == CLAW2_BC_CUSTOM || p->bc_upper[d] == CLAW2_BC_CUSTOM) return false;
+        if (!periodic_ok(p->bc_lower[d], p->bc_upper[d])) return false;
+    }
+    return p->mx >= 4 && p->my >= 4;
+}
+
+void tiles(const claw2_problem* p, int* nbx, int* nby)
+{
+    const bool split = p->transverse < 0;
+    const int tx = split ? STX : UTX, ty = split ? STY : UTY;
+    *nbx = (p->mx + tx - 1) / tx;
+    *nby = (p->my + ty - 1) / ty;
+}
+
+void fill_args(const claw2_problem* p, double* q, StepArgs& a)
+{
+    claw2_layout L;
+    claw2_get_layout(p, &L);
+    std::memset(&a, 0, sizeof a);
+    a.ld = L.ld; a.plane = L.plane;
+    a.mx = p->mx; a.my = p->my;
+    a.dx = p->dx; a.dy = p->dy;
+    a.order = p->order; a.trans = p->transverse; a.capa = p->index_capa; a.fwave = p->use_fwave;
+    a.limit_any = 0;
+    for (int w = 0; w < CLAW2_MAX_WAVES; w++) {
+        a.mthlim[w] = w < p->num_waves ? p->mthlim[w] : 0;
+        if (w < p->num_waves && p->mthlim[w] > 0) a.limit_any = 1;
+    }
+    for (int k = 0; k < CLAW2_MAX_PARAMS; k++) a.prm[k] = p->params[k];
+    a.ghost_fused = fused_ghosts(p) ? 1 : 0;
+    for (int d = 0; d < 2; d++) { a.bcl[d] = p->bc_lower[d]; a.bcu[d] = p->bc_upper[d]; }
+    (void)q;
+}
+
+template <class RP, bool SPLIT>
+int launch_step_t(const StepArgs& a, int nbx, int nby, cudaStream_t st)
+{
+    constexpr int TX = SPLIT ? STX : UTX, TY = SPLIT ? STY : UTY, NT = SPLIT ? SNT : UNT;
+    using SM = TileSmem<RP, TX, TY, NT, SPLIT>;
+    auto kern = step_kernel<RP, TX, TY, NT, SPLIT>;
+    static bool configured = false;
+    if (!configured) {
+        if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SM::bytes) != cudaSuccess)
+            return CLAW2_ERR_CUDA;
+        configured = true;
+    }
+    kern<<<dim3(nbx, nby), NT, SM::bytes, st>>>(a);
+    return cudaGetLastError() == cudaSuccess ? CLAW2_OK : CLAW2_ERR_CUDA;
+}
+
+int launch_step(const claw2_problem* p, const StepArgs& a, cudaStream_t st)
+{
+    int nbx, nby;
+    tiles(p, &nbx, &nby);
+    const bool split = p->transverse < 0;
+    switch (p->rp) {
+    case CLAW2_RP_ACOUSTICS:
+        return split ? launch_step_t<RpAcoustics, true>(a, nbx, nby, st) : launch_step_t<RpAcoustics, false>(a, nbx, nby, st);
+    case CLAW2_RP_VC_ACOUSTICS:
+        return split ? launch_step_t<RpVcAcoustics, true>(a, nbx, nby, st) : launch_step_t<RpVcAcoustics, false>(a, nbx, nby, st);
+    case CLAW2_RP_EULER_4WAVE:
+        return split ? launch_step_t<RpEuler<false>, true>(a, nbx, nby, st) : launch_step_t<RpEuler<false>, false>(a, nbx, nby, st);
+    case CLAW2_RP_EULER_5WAVE:
+        return split ? launch_step_t<RpEuler<true>, true>(a, nbx, nby, st) : launch_step_t<RpEuler<true>, false>(a, nbx, nby, st);
+    case CLAW2_RP_SHALLOW_ROE:
+        return split ? launch_step_t<RpShallow, true>(a, nbx, nby, st) : launch_step_t<RpShallow, false>(a, nbx, nby, st);
+    default:
+        return CLAW2_ERR_INVALID;
+    }
+}
+
+int launch_fill(const claw2_problem* p, double* q, int ncomp, const int* bl, const int* bu, bool is_aux,
+                double* q0, double* q1, const claw2_control* ctrl, cudaStream_t st)
+{
+    claw2_layout L;
+    claw2_get_layout(p, &L);
+    for (int axis = 0; axis < 2; axis++) {
+        FillArgs f;
+        f.q = q; f.ld = L.ld; f.plane = L.plane; f.mx = p->mx; f.my = p->my; f.ncomp = ncomp;
+        f.bl = bl[axis]; f.bu = bu[axis];
+        f.negate = is_aux ? -1 : axis + 1;
+        const int other = (axis == 0 ? p->my : p->mx) + 2 * CLAW2_NUM_GHOST;
+        const long long total = (long long)ncomp * other * 2 * CLAW2_NUM_GHOST;
+        const int threads = 256;
+        const int blocks = (int)((total + threads - 1) / threads);
+        if (ctrl) {
+            if (axis == 0) fill_kernel_ctrl<0><<<blocks, threads, 0, st>>>(f, q0, q1, ctrl);
+            else fill_kernel_ctrl<1><<<blocks, threads, 0, st>>>(f, q0, q1, ctrl);
+        } else {
+            if (axis == 0) fill_kernel<0><<<blocks, threads, 0, st>>>(f);
+            else fill_kernel<1><<<blocks, threads, 0, st>>>(f);
+        }
+        if (cudaGetLastError() != cudaSuccess) return CLAW2_ERR_CUDA;
+    }
+    return CLAW2_OK;
+}
+
+int conv(const claw2_problem* p, int ncomp, const double* src, double* dst, bool to_dev, bool ghosts, cudaStream_t st)
+{
+    claw2_layout L;
+    int rc = claw2_get_layout(p, &L);
+    if (rc) return rc;
+    const int g = ghosts ? 2 * CLAW2_NUM_GHOST : 0;
+    const int nx = p->mx + g, ny = p->my + g;
+    const long long total = (long long)ncomp * nx * ny;
+    const int threads = 256;
+    int blocks = (int)((total + threads - 1) / threads);
+    if (blocks > 148 * 32) blocks = 148 * 32;
+    if (blocks < 1) blocks = 1;
+    if (to_dev) ref_to_dev_kernel<<<blocks, threads, 0, st>>>(src, dst, ncomp, nx, ny, L.ld, L.plane, ghosts ? 1 : 0);
+    else dev_to_ref_kernel<<<blocks, threads, 0, st>>>(src, dst, ncomp, nx, ny, L.ld, L.plane, ghosts ? 1 : 0);
+    return cudaGetLastError() == cudaSuccess ? CLAW2_OK : CLAW2_ERR_CUDA;
+}
+
+}  // namespace
+
+// ===========================================================================
+// extern "C" ABI
+// ===========================================================================
+extern "C" {
+
+int claw2_abi_version(void) { return CLAW2_ABI_VERSION; }
+
+const char* claw2_strerror(int status)
+{
+    switch (status) {
+    case CLAW2_OK: return "ok";
+    case CLAW2_ERR_INVALID: return "invalid problem description or argument";
+    case CLAW2_ERR_UNSUPPORTED: return "feature not supported by this build";
+    case CLAW2_ERR_CUDA: return "CUDA runtime error";
+    case CLAW2_ERR_CFL: return "CFL too large, giving up!";
+    case CLAW2_ERR_MAX_STEPS: return "Maximum number of timesteps have been taken";
+    case CLAW2_ERR_NONFINITE: return "non-finite or non-physical state produced";
+    case CLAW2_ERR_TIMEOUT: return "bounded device wait gave up";
+    case CLAW2_ERR_NOMEM: return "out of memory";
+    case CLAW2_ERR_SIZE: return "size beyond the documented maximum";
+    default: return "unknown claw2 status";
+    }
+}
+
+int claw2_validate(const claw2_problem* p)
+{
+    int meqn, mw, maux;
+    if (!p) return CLAW2_ERR_INVALID;
+    if (solver_shape(p->rp, &meqn, &mw, &maux)) return CLAW2_ERR_INVALID;
+    if (p->num_eqn != meqn || p->num_waves != mw || p->num_aux < maux) return CLAW2_ERR_INVALID;
+    if (p->num_ghost != CLAW2_NUM_GHOST) return CLAW2_ERR_UNSUPPORTED;
+    if (p->mx < 2 || p->my < 2) return CLAW2_ERR_INVALID;
+    if (p->num_aux < 0 || p->num_aux > CLAW2_MAX_EQN) return CLAW2_ERR_INVALID;
+    if (p->order < 1 || p->order > 2) return CLAW2_ERR_INVALID;
+    if (p->transverse < -1 || p->transverse > 2) return CLAW2_ERR_INVALID;
+    if (p->index_capa < -1 || p->index_capa >= p->num_aux) return CLAW2_ERR_INVALID;
+    if (!(p->dx > 0.0) || !(p->dy > 0.0)) return CLAW2_ERR_INVALID;
+    for (int w = 0; w < p->num_waves; w++)
+        if (p->mthlim[w] < 0) return CLAW2_ERR_INVALID;
+    for (int d = 0; d < 2; d++) {
+        if (p->bc_lower[d] < 0 || p->bc_lower[d] > 3 || p->bc_upper[d] < 0 || p->bc_upper[d] > 3) return CLAW2_ERR_INVALID;
+        if (!periodic_ok(p->bc_lower[d], p->bc_upper[d])) return CLAW2_ERR_UNSUPPORTED;
+        if (p->num_aux > 0 && (p->aux_bc_lower[d] < 0 || p->aux_bc_lower[d] > 3 ||
+                               p->aux_bc_upper[d] < 0 || p->aux_bc_upper[d] > 3)) return CLAW2_ERR_INVALID;
+    }
+    return CLAW2_OK;
+}
+
+int claw2_get_layout(const claw2_problem* p, claw2_layout* out)
+{
+    if (!p || !out || p->mx < 1 || p->my < 1) return CLAW2_ERR_INVALID;
+    const long long nx = (long long)p->mx + 2 * CLAW2_NUM_GHOST;
+    out->ld = (nx + 15) / 16 * 16;              // 128-byte row pitch
+    out->rows = (long long)p->my + 2 * CLAW2_NUM_GHOST;
+    out->plane = out->ld * out->rows;
+    out->q_elems = (long long)p->num_eqn * out->plane;
+    out->aux_elems = (long long)p->num_aux * out->plane;
+    return CLAW2_OK;
+}
+
+size_t claw2_scratch_bytes(const claw2_problem* p)
+{
+    if (!p || p->mx < 1 || p->my < 1) return 0;
+    int nbx, nby;
+    tiles(p, &nbx, &nby);
+    return 64 + sizeof(double) * (size_t)nbx * (size_t)nby;
+}
+
+int claw2_fill_ghosts(const claw2_problem* p, double* q, void* stream)
+{
+    int rc = claw2_validate(p);
+    if (rc) return rc;
+    return launch_fill(p, q, p->num_eqn, p->bc_lower, p->bc_upper, false, nullptr, nullptr, nullptr, S(stream));
+}
+
+int claw2_fill_aux_ghosts(const claw2_problem* p, double* aux, void* stream)
+{
+    int rc = claw2_validate(p);
+    if (rc) return rc;
+    if (p->num_aux == 0) return CLAW2_OK;
+    return launch_fill(p, aux, p->num_aux, p->aux_bc_lower, p->aux_bc_upper, true, nullptr, nullptr, nullptr, S(stream));
+}
+
+int claw2_step(const claw2_problem* p, const double* q_in, double* q_out, const double* aux, double dt,
+               void* scratch, double* cfl_dev, void* stream)
+{
+    int rc = claw2_validate(p);
+    if (rc) return rc;
+    if (!q_in || !q_out || !scratch || !cfl_dev || (p->num_aux > 0 && !aux) || q_in == q_out) return CLAW2_ERR_INVALID;
+    StepArgs a;
+    fill_args(p, q_out, a);
+    a.qin = q_in; a.qout = q_out; a.aux = aux; a.dt = dt;
+    a.ticket = static_cast<unsigned int*>(scratch);
+    a.partials = reinterpret_cast<double*>(static_cast<char*>(scratch) + 64);
+    a.cfl_out = cfl_dev;
+    if ((rc = launch_step(p, a, S(stream)))) return rc;
+    if (!a.ghost_fused)
+        return launch_fill(p, q_out, p->num_eqn, p->bc_lower, p->bc_upper, false, nullptr, nullptr, nullptr, S(stream));
+    return CLAW2_OK;
+}
+
+int claw2_advance(const claw2_problem* p, double* q0, double* q1, const double* aux, claw2_control* ctrl,
+                  void* scratch, int nsteps, void* stream)
+{
+    int rc = claw2_validate(p);
+    if (rc) return rc;
+    if (!q0 || !q1 || !ctrl || !scratch || (p->num_aux > 0 && !aux) || nsteps < 0) return CLAW2_ERR_INVALID;
+    StepArgs a;
+    fill_args(p, q0, a);
+    a.q0 = q0; a.q1 = q1; a.aux = aux; a.ctrl = ctrl;
+    a.ticket = static_cast<unsigned int*>(scratch);
+    a.partials = reinterpret_cast<double*>(static_cast<char*>(scratch) + 64);
+    for (int n = 0; n < nsteps; n++) {
+        if ((rc = launch_step(p, a, S(stream)))) return rc;
+        if (!a.ghost_fused &&
+            (rc = launch_fill(p, nullptr, p->num_eqn, p->bc_lower, p->bc_upper, false, q0, q1, ctrl, S(stream))))
+            return rc;
+    }
+    return CLAW2_OK;
+}
+
+int claw2_control_init(claw2_control* c, double t, double dt, double tend, double cfl_max, double cfl_desired,
+                       double dt_max, int dt_variable, int take_one_step, int64_t max_steps, double prev_cfl)
+{
+    if (!c) return CLAW2_ERR_INVALID;
+    std::memset(c, 0, sizeof *c);
+    c->t = t; c->dt = dt; c->tstart = t; c->tend = tend;
+    c->cfl = prev_cfl;
+    c->cfl_max = cfl_max; c->cfl_desired = cfl_desired; c->dt_max = dt_max;
+    c->status_cflmax = prev_cfl; c->status_dtmin = dt; c->status_dtmax = dt;
+    c->dt_variable = dt_variable; c->take_one_step = take_one_step;
+    c->max_steps = max_steps;
+    if (!dt_variable) {                                       // solver.py:618-624
+        if (take_one_step) c->max_steps = 1;
+        else {
+            c->max_steps = (int64_t)((tend - t + 1e-10) / dt);
+            if (std::fabs(c->max_steps * dt - (tend - t)) > 1e-5 * (tend - t)) return CLAW2_ERR_INVALID;
+        }
+    }
+    if (dt_variable && cfl_desired > cfl_max) return CLAW2_ERR_INVALID;   // :625-626
+    if (tend <= t && !take_one_step) c->max_steps = 0;                     // :627-629
+    if (c->max_steps <= 0) { c->done = 1; return CLAW2_OK; }
+    if (!take_one_step) {                                                  // :637-641
+        if (c->t + c->dt > c->tend && c->tstart < c->tend) c->dt = c->tend - c->t;
+        if (c->tend - c->t - c->dt < 1.e-14 * c->t) c->dt = c->tend - c->t;
+    }
+    return CLAW2_OK;
+}
+
+int claw2_ref_to_device(const claw2_problem* p, int ncomp, const double* ref, double* dev, void* stream)
+{
+    if (!p || !ref || !dev || ncomp < 1) return CLAW2_ERR_INVALID;
+    return conv(p, ncomp, ref, dev, true, true, S(stream));
+}
+
+int claw2_device_to_ref(const claw2_problem* p, int ncomp, const double* dev, double* ref, void* stream)
+{
+    if (!p || !ref || !dev || ncomp < 1) return CLAW2_ERR_INVALID;
+    return conv(p, ncomp, dev, ref, false, true, S(stream));
+}
+
+// ---------------------------------------------------------------------------
+// host-buffer session
+// ---------------------------------------------------------------------------
+struct claw2_session {
+    claw2_problem p;
+    claw2_layout L;
+    double *q0, *q1, *aux, *ref, *cfl;
+    void* scratch;
+    claw2_control* ctrl;       // device
+    claw2_control* ctrl_host;  // pinned
+    cudaStream_t stream;
+};
+
+int claw2_session_create(const claw2_problem* p, claw2_session** out)
+{
+    int rc = claw2_validate(p);
+    if (rc) return rc;
+    if (!out) return CLAW2_ERR_INVALID;
+    claw2_session* s = new (std::nothrow) claw2_session;
+    if (!s) return CLAW2_ERR_NOMEM;
+    std::memset(s, 0, sizeof *s);
+    s->p = *p;
+    claw2_get_layout(p, &s->L);
+    const size_t qb = sizeof(double) * s->L.q_elems;
+    const size_t nref = (size_t)(p->num_eqn > p->num_aux ? p->num_eqn : p->num_aux) *
+                        (p->mx + 2 * CLAW2_NUM_GHOST) * (p->my + 2 * CLAW2_NUM_GHOST);
+    bool ok = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) == cudaSuccess;
+    ok = ok && cudaMalloc(&s->q0, qb) == cudaSuccess && cudaMalloc(&s->q1, qb) == cudaSuccess;
+    ok = ok && cudaMalloc(&s->ref, sizeof(double) * nref) == cudaSuccess;
+    ok = ok && cudaMalloc(&s->cfl, sizeof(double)) == cudaSuccess;
+    ok = ok && cudaMalloc(&s->scratch, claw2_scratch_bytes(p)) == cudaSuccess;
+    ok = ok && cudaMalloc(&s->ctrl, sizeof(claw2_control)) == cudaSuccess;
+    ok = ok && cudaMallocHost(&s->ctrl_host, sizeof(claw2_control)) == cudaSuccess;
+    if (ok && p->num_aux > 0) ok = cudaMalloc(&s->aux, sizeof(double) * s->L.aux_elems) == cudaSuccess;
+    ok = ok && cudaMemset(s->q0, 0, qb) == cudaSuccess && cudaMemset(s->q1, 0, qb) == cudaSuccess;
+    ok = ok && cudaMemset(s->scratch, 0, claw2_scratch_bytes(p)) == cudaSuccess;
+    if (!ok) { claw2_session_destroy(s); return CLAW2_ERR_NOMEM; }
+    *out = s;
+    return CLAW2_OK;
+}
+
+int claw2_session_destroy(claw2_session* s)
+{
+    if (!s) return CLAW2_OK;
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    cudaFree(s->q0); cudaFree(s->q1); cudaFree(s->ref); cudaFree(s->cfl); cudaFree(s->scratch);
+    cudaFree(s->ctrl); cudaFree(s->aux);
+    if (s->ctrl_host) cudaFreeHost(s->ctrl_host);
+    if (s->stream) cudaStreamDestroy(s->stream);
+    delete s;
+    return CLAW2_OK;
+}
+
+static int upload_aux(claw2_session* s, const double* aux, bool ghosts)
+{
+    const claw2_problem* p = &s->p;
+    if (p->num_aux == 0) return CLAW2_OK;
+    if (!aux) return CLAW2_ERR_INVALID;
+    const size_t n = (size_t)p->num_aux * (p->mx + (ghosts ? 2 * CLAW2_NUM_GHOST : 0)) *
+                     (p->my + (ghosts ? 2 * CLAW2_NUM_GHOST : 0));
+    if (cudaMemcpyAsync(s->ref, aux, n * sizeof(double), cudaMemcpyHostToDevice, s->stream) != cudaSuccess)
+        return CLAW2_ERR_CUDA;
+    int rc = conv(p, p->num_aux, s->ref, s->aux, true, ghosts, s->stream);
+    if (rc) return rc;
+    if (!ghosts) return claw2_fill_aux_ghosts(p, s->aux, s->stream);
+    return CLAW2_OK;
+}
+
+int claw2_session_step2(claw2_session* s, const double* qold, double* qnew, const double* aux, double dt,
+                        double* cfl)
+{
+    if (!s || !qold || !qnew || !cfl) return CLAW2_ERR_INVALID;
+    const claw2_problem* p = &s->p;
+    const size_t n = (size_t)p->num_eqn * (p->mx + 2 * CLAW2_NUM_GHOST) * (p->my + 2 * CLAW2_NUM_GHOST);
+    int rc;
+    if ((rc = upload_aux(s, aux, true))) return rc;
+    if (cudaMemcpyAsync(s->ref, qold, n * sizeof(double), cudaMemcpyHostToDevice, s->stream) != cudaSuccess)
+        return CLAW2_ERR_CUDA;
+    if ((rc = conv(p, p->num_eqn, s->ref, s->q0, true, true, s->stream))) return rc;
+    if ((rc = claw2_step(p, s->q0, s->q1, s->aux, dt, s->scratch, s->cfl, s->stream))) return rc;
+    if ((rc = conv(p, p->num_eqn, s->q1, s->ref, false, true, s->stream))) return rc;
+    if (cudaMemcpyAsync(qnew, s->ref, n * sizeof(double), cudaMemcpyDeviceToHost, s->stream) != cudaSuccess)
+        return CLAW2_ERR_CUDA;
+    if (cudaMemcpyAsync(cfl, s->cfl, sizeof(double), cudaMemcpyDeviceToHost, s->stream) != cudaSuccess)
+        return CLAW2_ERR_CUDA;
+    if (cudaStreamSynchronize(s->stream) != cudaSuccess) return CLAW2_ERR_CUDA;
+    return std::isnan(*cfl) ? CLAW2_ERR_NONFINITE : CLAW2_OK;
+}
+
+int claw2_session_evolve(claw2_session* s, double* q, const double* aux, double* t, double* dt, double tend,
+                         double cfl_max, double cfl_desired, double dt_max, int64_t max_steps, double* status)
+{
+    if (!s || !q || !t || !dt) return CLAW2_ERR_INVALID;
+    const claw2_problem* p = &s->p;
+    const size_t n = (size_t)p->num_eqn * p->mx * p->my;
+    int rc;
+    if ((rc = upload_aux(s, aux, false))) return rc;
+    if (cudaMemcpyAsync(s->ref, q, n * sizeof(double), cudaMemcpyHostToDevice, s->stream) != cudaSuccess)
+        return CLAW2_ERR_CUDA;
+    if ((rc = conv(p, p->num_eqn, s->ref, s->q0, true, false, s->stream))) return rc;
+    if ((rc = claw2_fill_ghosts(p, s->q0, s->stream))) return rc;
+    if ((rc = claw2_control_init(s->ctrl_host, *t, *dt, tend, cfl_max, cfl_desired, dt_max, 1, 0, max_steps, cfl_desired)))
+        return rc;
+    if (cudaMemcpyAsync(s->ctrl, s->ctrl_host, sizeof(claw2_control), cudaMemcpyHostToDevice, s->stream) != cudaSuccess)
+        return CLAW2_ERR_CUDA;
+    const int batch = 16;
+    for (;;) {
+        if ((rc = claw2_advance(p, s->q0, s->q1, s->aux, s->ctrl, s->scratch, batch, s->stream))) return rc;
+        if (cudaMemcpyAsync(s->ctrl_host, s->ctrl, sizeof(claw2_control), cudaMemcpyDeviceToHost, s->stream) != cudaSuccess)
+            return CLAW2_ERR_CUDA;
+        if (cudaStreamSynchronize(s->stream) != cudaSuccess) return CLAW2_ERR_CUDA;
+        if (s->ctrl_host->done) break;
+    }
+    const claw2_control* c = s->ctrl_host;
+    double* cur = c->cur ? s->q1 : s->q0;
+    if ((rc = conv(p, p->num_eqn, cur, s->ref, false, false, s->stream))) return rc;
+    if (cudaMemcpyAsync(q, s->ref, n * sizeof(double), cudaMemcpyDeviceToHost, s->stream) != cudaSuccess)
+        return CLAW2_ERR_CUDA;
+    if (cudaStreamSynchronize(s->stream) != cudaSuccess) return CLAW2_ERR_CUDA;
+    *t = c->t;
+    *dt = c->dt;
+    if (status) {
+        status[0] = c->status_cflmax; status[1] = c->status_dtmin; status[2] = c->status_dtmax;
+        status[3] = (double)c->numsteps; status[4] = (double)c->rejected;
+    }
+    return c->error;
+}
+
+}  // extern "C"

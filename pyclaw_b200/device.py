@@ -1,0 +1,159 @@
+"""Device-resident state of one ClawSolver2D: buffers held as torch tensors,
+kernels launched through the C ABI of libclaw2.so on torch's current stream.
+
+Buffers (device layout of include/claw2.h, ghost cells included):
+  q[0], q[1]  ping-pong state buffers; control.cur says which one is current
+  aux         auxiliary fields, ghost cells filled once per upload
+  scratch     per-CTA CFL partials + block-arrival counter
+  ctrl        claw2_control (device-side time-step controller)
+"""
+import ctypes
+
+import numpy as np
+
+from . import _abi
+from . import _lib
+
+
+def _torch():
+    import torch
+    return torch
+
+
+class DeviceState(object):
+    def __init__(self, problem, device=None):
+        torch = _torch()
+        if not torch.cuda.is_available():
+            raise _lib.ClawLibraryError("pyclaw_b200 needs a CUDA device (sm_100a); none is available")
+        self.lib = _lib.load()
+        self.p = problem
+        _lib.check(self.lib.claw2_validate(ctypes.byref(problem)), "claw2_validate")
+        self.L = _lib.layout(problem)
+        self.device = torch.device(device if device is not None else "cuda")
+        f64 = dict(dtype=torch.float64, device=self.device)
+        self.q = [torch.zeros(self.L.q_elems, **f64), torch.zeros(self.L.q_elems, **f64)]
+        self.aux = torch.zeros(max(self.L.aux_elems, 1), **f64)
+        nscr = int(self.lib.claw2_scratch_bytes(ctypes.byref(problem)))
+        self.scratch = torch.zeros((nscr + 7) // 8 * 8, dtype=torch.uint8, device=self.device)
+        self.ctrl = torch.zeros(ctypes.sizeof(_abi.Control), dtype=torch.uint8, device=self.device)
+        self.ctrl_host = torch.zeros(ctypes.sizeof(_abi.Control), dtype=torch.uint8).pin_memory()
+        self.cfl_dev = torch.zeros(1, **f64)
+        self.cur = 0
+        self.device_newer = False       # device q changed since the last download
+        self.host_dirty = True          # host q may differ from the device copy
+        self.aux_dirty = True
+        self.state = None
+
+    # ---- plumbing ----------------------------------------------------------
+    @property
+    def stream(self):
+        return ctypes.c_void_p(_torch().cuda.current_stream(self.device).cuda_stream)
+
+    def ptr(self, t):
+        return ctypes.c_void_p(t.data_ptr())
+
+    def qview(self, k):
+        return self.q[k].view(self.p.num_eqn, self.L.rows, self.L.ld)
+
+    def interior(self, k):
+        g = _abi.NUM_GHOST
+        return self.qview(k)[:, g:g + self.p.my, g:g + self.p.mx]
+
+    # ---- host <-> device -------------------------------------------------
+    def attach(self, state):
+        self.state = state
+        state._dev = self
+
+    def host_q_touched(self):
+        self.host_dirty = True
+
+    def host_aux_touched(self):
+        self.aux_dirty = True
+
+    def refresh_host_q(self, state):
+        if self.device_newer:
+            state._q = self.download_q()
+            self.device_newer = False
+
+    def download_q(self):
+        v = self.interior(self.cur).permute(0, 2, 1).cpu().numpy()
+        return np.asfortranarray(v)
+
+    def upload_q(self, q):
+        torch = _torch()
+        src = torch.from_numpy(np.ascontiguousarray(np.asarray(q, dtype=np.float64).transpose(0, 2, 1)))
+        self.interior(self.cur).copy_(src)
+        _lib.check(self.lib.claw2_fill_ghosts(ctypes.byref(self.p), self.ptr(self.q[self.cur]), self.stream),
+                   "claw2_fill_ghosts")
+
+    def upload_aux(self, aux):
+        if self.p.num_aux == 0:
+            return
+        torch = _torch()
+        g = _abi.NUM_GHOST
+        v = self.aux[:self.L.aux_elems].view(self.p.num_aux, self.L.rows, self.L.ld)
+        src = torch.from_numpy(np.ascontiguousarray(np.asarray(aux, dtype=np.float64).transpose(0, 2, 1)))
+        v[:, g:g + self.p.my, g:g + self.p.mx].copy_(src)
+        _lib.check(self.lib.claw2_fill_aux_ghosts(ctypes.byref(self.p), self.ptr(self.aux), self.stream),
+                   "claw2_fill_aux_ghosts")
+
+    def sync_from_host(self):
+        """Upload whatever the host side may have changed since the last step."""
+        st = self.state
+        if self.aux_dirty:
+            if st._aux is not None:
+                self.upload_aux(st._aux)
+            self.aux_dirty = False
+        if self.host_dirty:
+            self.upload_q(st._q)
+            self.host_dirty = False
+            self.device_newer = False
+
+    def ghosted_ref(self):
+        """Current q with ghost cells, in the reference layout (num_eqn, mx+4, my+4), on the host."""
+        v = self.qview(self.cur)[:, :, :self.p.mx + 2 * _abi.NUM_GHOST].permute(0, 2, 1).cpu().numpy()
+        return np.asfortranarray(v)
+
+    def set_ghosted_ref(self, qbc, k=None):
+        torch = _torch()
+        k = self.cur if k is None else k
+        src = torch.from_numpy(np.ascontiguousarray(np.asarray(qbc).transpose(0, 2, 1)))
+        self.qview(k)[:, :, :self.p.mx + 2 * _abi.NUM_GHOST].copy_(src)
+
+    # ---- stepping ---------------------------------------------------------
+    def step(self, dt):
+        """One step q[cur] -> q[1-cur] with explicit dt; returns the CFL number."""
+        nxt = 1 - self.cur
+        _lib.check(self.lib.claw2_step(ctypes.byref(self.p), self.ptr(self.q[self.cur]), self.ptr(self.q[nxt]),
+                                       self.ptr(self.aux), float(dt), self.ptr(self.scratch),
+                                       self.ptr(self.cfl_dev), self.stream), "claw2_step")
+        cfl = float(self.cfl_dev.item())
+        return cfl, nxt
+
+    def evolve(self, control, max_batch=64):
+        """Run the device-controlled loop until control is done; returns the final Control."""
+        torch = _torch()
+        control.cur = self.cur
+        host = _abi.Control.from_address(self.ctrl_host.data_ptr())
+        ctypes.memmove(ctypes.addressof(host), ctypes.addressof(control), ctypes.sizeof(control))
+        self.ctrl.copy_(self.ctrl_host, non_blocking=True)
+        stream = torch.cuda.current_stream(self.device)
+        batch = 8
+        while True:
+            _lib.check(self.lib.claw2_advance(ctypes.byref(self.p), self.ptr(self.q[0]), self.ptr(self.q[1]),
+                                              self.ptr(self.aux), self.ptr(self.ctrl), self.ptr(self.scratch),
+                                              int(batch), self.stream), "claw2_advance")
+            self.ctrl_host.copy_(self.ctrl, non_blocking=True)
+            stream.synchronize()
+            if host.done:
+                break
+            if host.dt > 0:
+                remaining = (host.tend - host.t) / host.dt
+                batch = int(max(1, min(max_batch, remaining + 1)))
+            else:
+                batch = max_batch
+        out = _abi.Control()
+        ctypes.memmove(ctypes.addressof(out), ctypes.addressof(host), ctypes.sizeof(out))
+        self.cur = out.cur
+        self.device_newer = True
+        return out

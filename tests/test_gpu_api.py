@@ -1,0 +1,216 @@
+"""GPU runs through the public pyclaw_b200 API (Controller.run /
+ClawSolver2D.evolve_to_time), checked against the oracle's replay of the
+reference driver loop and against the reference's own golden files."""
+import os
+
+import numpy as np
+import pytest
+
+import kat_setups as K
+import pyclaw_b200 as pc
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def _api_run(p, q, aux, run, tfinal, nout, split, trans=2, rp=None, bcs=None, src=None, keep=True,
+             bounds=((0.0, 1.0), (0.0, 1.0))):
+    """Build the same problem through the public API and run it on the GPU."""
+    x = pc.Dimension('x', bounds[0][0], bounds[0][1], p.mx)
+    y = pc.Dimension('y', bounds[1][0], bounds[1][1], p.my)
+    assert x.delta == p.dx and y.delta == p.dy
+    domain = pc.Domain([x, y])
+    state = pc.State(domain, p.num_eqn, p.num_aux)
+    state.q[...] = q
+    if p.num_aux:
+        state.aux[...] = aux
+    solver = pc.ClawSolver2D(rp)
+    names = {1: ('rho', 'bulk', 'cc', 'zz'), 3: ('gamma', 'gamma1'), 4: ('gamma', 'gamma1'), 5: ('grav',)}
+    for k, key in enumerate(names.get(p.rp, ())):
+        state.problem_data[key] = p.params[k]
+    solver.dimensional_split = split
+    solver.transverse_waves = trans
+    solver.limiters = [int(p.mthlim[w]) for w in range(p.num_waves)]
+    solver.bc_lower = [int(p.bc_lower[0]), int(p.bc_lower[1])]
+    solver.bc_upper = [int(p.bc_upper[0]), int(p.bc_upper[1])]
+    solver.aux_bc_lower = [int(p.aux_bc_lower[0]), int(p.aux_bc_lower[1])]
+    solver.aux_bc_upper = [int(p.aux_bc_upper[0]), int(p.aux_bc_upper[1])]
+    solver.cfl_max = run['cfl_max']
+    solver.cfl_desired = run['cfl_desired']
+    solver.dt_initial = run['dt_initial']
+    if bcs:
+        solver.user_bc_lower = bcs
+    if src:
+        solver.step_source = src
+    claw = pc.Controller()
+    claw.solution = pc.Solution(state, domain)
+    claw.solver = solver
+    claw.tfinal = tfinal
+    claw.num_output_times = nout
+    claw.output_format = None
+    claw.keep_copy = keep
+    claw.run()
+    return claw, solver
+
+
+def test_vc_acoustics_app_matches_golden_and_oracle(orc):
+    """apps/acoustics_2d_variable: unsplit, trans=1, walls, rejected first step."""
+    p, q, aux, run = K.acoustics_variable_setup()
+    claw, solver = _api_run(p, q, aux, run, 0.6, 20, split=False, trans=1, rp=pc.riemann.rp2_vc_acoustics,
+                            bounds=((-1.0, 1.0), (-1.0, 1.0)))
+    ref = orc.Run(p, q, aux, omp=True, **run)
+    frames = ref.run(0.6, num_output_times=20)
+    got = claw.frames[20].state.q
+    assert np.array_equal(got, frames[20])
+    gold = np.load(os.path.join(GOLD, "vc_acoustics_pressure.npz"))["pressure"]
+    assert np.max(np.abs(gold - got[0])) < 1e-13
+    io = np.load(os.path.join(GOLD, "vc_acoustics_io.npz"))
+    assert K.check_diff(io["q20"], got, reltol=1e-4) is None
+
+
+def test_acoustics_homogeneous_split_app(orc):
+    p, q, aux, run = K.acoustics_homogeneous_setup()
+    claw, solver = _api_run(p, q, aux, run, 0.12, 10, split=True, rp=pc.riemann.rp2_acoustics,
+                            bounds=((-1.0, 1.0), (-1.0, 1.0)))
+    ref = orc.Run(p, q, aux, **run)
+    frames = ref.run(0.12, num_output_times=10)
+    got = claw.frames[-1].state.q
+    assert np.array_equal(got, frames[-1])
+    gold = np.load(os.path.join(GOLD, "acoustics_pressure.npz"))["pressure"]
+    assert K.check_diff(gold, got[0], reltol=1e-3) is None
+
+
+def test_shockbubble_app_custom_bc_and_source(orc):
+    """apps/euler_2d/shockbubble.py: custom inflow BC and a Python source term run
+    through the host-driven loop; abstol 1e-12 against the reference's file."""
+    p, q, aux, run, bcs, src = K.shockbubble_setup()
+    cb = bcs[(0, "lower")]
+
+    def user_bc(state, dim, t, qbc, num_ghost):
+        if dim.name == 'x':
+            cb(qbc, t)
+
+    def step_source(solver, state, dt):
+        src(state.q, dt)
+
+    claw, solver = _api_run(p, q, aux, run, 0.2, 1, split=True, rp=pc.riemann.rp2_euler_5wave,
+                            bcs=user_bc, src=step_source, bounds=((0.0, 2.0), (0.0, 0.5)))
+    got = claw.frames[1].state.q
+    ref = orc.Run(p, q, aux, bc_callbacks=bcs, step_source=src, **run)
+    frames = ref.run(0.2, num_output_times=1)
+    assert np.array_equal(got, frames[1])
+    gold = np.load(os.path.join(GOLD, "shockbubble_density.npz"))["density"]
+    assert K.check_diff(0, np.linalg.norm(gold - got[0]), abstol=1e-12) is None
+
+
+def test_config1_acoustics_full_run_parity(orc):
+    """256x256 acoustics, walls, unsplit trans=2, MC, cfl 0.9, to t=0.6: the
+    whole device-controlled run must equal the oracle cell for cell (the bar
+    is 1e-11 relative; the result is identical), with the same dt sequence,
+    and mass must be conserved to round-off."""
+    import bench
+    p, q, aux, run, tfinal = bench.acoustics_config()
+    claw, solver = _api_run(p, q, aux, run, tfinal, 1, split=False, trans=2, rp=pc.riemann.rp2_acoustics,
+                            bounds=((-1.0, 1.0), (-1.0, 1.0)))
+    got = claw.solution.state.q
+    ref = orc.Run(p, q, aux, omp=True, **run)
+    ref.run(tfinal, num_output_times=1, keep_copy=False)
+    rel = np.max(np.abs(got - ref.q)) / np.max(np.abs(ref.q))
+    assert rel <= 1e-11, rel
+    assert np.array_equal(got, ref.q)
+    assert solver.status['numsteps'] == ref.steps_taken and claw.solution.t == ref.t
+    mass0 = np.sum(q[0])
+    assert abs(np.sum(got[0]) - mass0) <= 1e-12 * max(1.0, abs(mass0)) * p.mx
+
+
+def test_config2_shockbubble_reduced_full_run(orc):
+    """The shock-bubble workload at 320x80 (a quarter of the benchmark's
+    resolution per axis) run to t=0.6: identical to the oracle."""
+    import bench
+    p, q, aux, run, tfinal = bench.shockbubble_config(320, 80)
+    claw, solver = _api_run(p, q, aux, run, tfinal, 1, split=False, trans=2, rp=pc.riemann.rp2_euler_4wave,
+                            bounds=((0.0, 2.0), (0.0, 0.5)))
+    got = claw.solution.state.q
+    ref = orc.Run(p, q, aux, omp=True, **run)
+    ref.run(tfinal, num_output_times=1, keep_copy=False)
+    assert np.array_equal(got, ref.q), np.max(np.abs(got - ref.q))
+    assert solver.status['numsteps'] == ref.steps_taken
+
+
+def test_config2_full_size_first_steps(orc):
+    """1280x320 shock bubble: the first 12 device-controlled steps equal the oracle."""
+    import bench
+    p, q, aux, run, tfinal = bench.shockbubble_config()
+    x = pc.Dimension('x', 0.0, 2.0, p.mx)
+    y = pc.Dimension('y', 0.0, 0.5, p.my)
+    domain = pc.Domain([x, y])
+    state = pc.State(domain, 4)
+    state.problem_data['gamma'] = 1.4
+    state.problem_data['gamma1'] = 1.4 - 1.0
+    state.q[...] = q
+    solver = bench.make_solver(pc, p, run)
+    sol = pc.Solution(state, domain)
+    solver.setup(sol)
+    solver.dt = run['dt_initial']
+    ref = orc.Run(p, q, aux, omp=True, **run)
+    for _ in range(12):
+        solver.evolve_to_time(sol)          # one step (take_one_step)
+        ref.evolve_to_time(None)
+        assert solver.dt == ref.dt and sol.t == ref.t
+    assert np.array_equal(sol.state.q, ref.q)
+
+
+def test_walled_euler_conserves_mass_and_energy():
+    import bench
+    p, q, aux, run, tfinal = bench.shockbubble_config(320, 80, walls=True)
+    claw, solver = _api_run(p, q, aux, run, 0.2, 1, split=False, trans=2, rp=pc.riemann.rp2_euler_4wave,
+                            bounds=((0.0, 2.0), (0.0, 0.5)))
+    got = claw.solution.state.q
+    for m in (0, 3):
+        s0, s1 = np.sum(q[m]), np.sum(got[m])
+        assert abs(s1 - s0) <= 64 * np.finfo(float).eps * np.sum(np.abs(q[m])) * 10, (m, s1 - s0)
+
+
+def test_fixed_dt_too_large_gives_up():
+    p, q, aux, run = K.acoustics_homogeneous_setup(mx=40, my=40, split=False)
+    x = pc.Dimension('x', -1.0, 1.0, 40)
+    y = pc.Dimension('y', -1.0, 1.0, 40)
+    domain = pc.Domain([x, y])
+    state = pc.State(domain, 3)
+    state.problem_data.update(rho=1.0, bulk=4.0, cc=2.0, zz=2.0)
+    state.q[...] = q
+    solver = pc.ClawSolver2D(pc.riemann.rp2_acoustics)
+    solver.dimensional_split = False
+    solver.bc_lower = [pc.BC.extrap] * 2
+    solver.bc_upper = [pc.BC.extrap] * 2
+    solver.dt_variable = False
+    solver.dt_initial = 0.1
+    solver.dt = 0.1
+    sol = pc.Solution(state, domain)
+    with pytest.raises(Exception, match="CFL too large, giving up!"):
+        solver.evolve_to_time(sol, 0.2)
+
+
+def test_session_step2_host_buffers(orc):
+    """The f2py-shaped entry point: reference-layout host arrays in and out."""
+    import ctypes
+    import gpu_helpers as H
+    from pyclaw_b200 import _lib
+    lib = _lib.load()
+    p = H.problem("euler4", 45, 33, 2)
+    q, _ = H.init_fields(p)
+    qbc = orc.new_qbc(p, q)
+    orc.fill_ghosts(p, qbc)
+    s = ctypes.c_void_p()
+    _lib.check(lib.claw2_session_create(ctypes.byref(p), ctypes.byref(s)), "session_create")
+    try:
+        qnew = qbc.copy(order="F")
+        cfl = ctypes.c_double()
+        _lib.check(lib.claw2_session_step2(s, qbc.ctypes.data, qnew.ctypes.data, None, 0.003, ctypes.byref(cfl)),
+                   "session_step2")
+        ref = qbc.copy(order="F")
+        cref = orc.step_hyperbolic(p, ref, None, 0.003)
+        assert cfl.value == cref
+        assert np.array_equal(qnew[:, 2:-2, 2:-2], ref[:, 2:-2, 2:-2])
+    finally:
+        lib.claw2_session_destroy(s)
