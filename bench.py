@@ -146,7 +146,7 @@ class ClockSampler(object):
             os.makedirs(os.path.dirname(self.path), exist_ok=True)
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), "--query-gpu=" + self.QUERY,
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                          "--format=csv,noheader,nounits", "-lms", "20"],
                                          stdout=self.f, stderr=subprocess.DEVNULL)
         except (OSError, FileNotFoundError):
             self.proc = None
@@ -337,6 +337,7 @@ def run_ours(args, world, rank, local):
     clocks = ClockSampler(torch.cuda.current_device()) if rank == 0 or world > 1 else None
     if clocks:
         clocks.start()
+        time.sleep(0.3)                       # let the sampler start before the timed region
     _barrier(world)
     torch.cuda.synchronize()
     w0 = time.perf_counter()
@@ -451,7 +452,7 @@ def _e2e(lib, prob, q, run, args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")

@@ -27,6 +27,7 @@ struct DevCtx {
     __device__ __forceinline__ int nbx() const { return gridDim.x; }
     __device__ __forceinline__ int nby() const { return gridDim.y; }
     __device__ __forceinline__ void sync() const { __syncthreads(); }
+    __device__ __forceinline__ void syncwarp() const { __syncwarp(); }
     __device__ __forceinline__ void fence() const { __threadfence(); }
     __device__ __forceinline__ unsigned atomic_inc(unsigned* p) const { return atomicAdd(p, 1u); }
     __device__ __forceinline__ double load_volatile(const double* p) const { return *(volatile const double*)p; }
@@ -34,8 +35,12 @@ struct DevCtx {
     __device__ __forceinline__ double* smem() const { return sm; }
 };
 
+#ifndef CLAW2_MINB
+#define CLAW2_MINB 2        // resident CTAs per SM the register budget is sized for
+#endif
+
 template <class RP, int TX, int TY, int NT, bool SPLIT>
-__global__ void __launch_bounds__(NT) step_kernel(StepArgs a)
+__global__ void __launch_bounds__(NT, CLAW2_MINB) step_kernel(StepArgs a)
 {
     extern __shared__ double smem_dyn[];
     DevCtx ctx{smem_dyn};
@@ -43,7 +48,10 @@ __global__ void __launch_bounds__(NT) step_kernel(StepArgs a)
 }
 
 // Tile shapes: a line of a chunk has 32 interface slots, so TX+3, TY+3 <= 32.
-constexpr int UTX = 29, UTY = 29, UNT = 256;   // unsplit
+#ifndef CLAW2_UNT
+#define CLAW2_UNT 256
+#endif
+constexpr int UTX = 29, UTY = 29, UNT = CLAW2_UNT;   // unsplit
 constexpr int STX = 28, STY = 28, SNT = 256;   // dimensional splitting
 
 // ---------------------------------------------------------------------------

@@ -187,48 +187,69 @@ CLAW2_HD void write_cell(const StepArgs& a, double* qo, int i, int j, const doub
 template <int A, int B> struct CMax { static constexpr int value = A > B ? A : B; };
 
 // Shared-memory footprint of the tile kernels (doubles).
+//   Qx   the tile's state after the x sweep (then the final state)
+//   WB   per interface slot: waves and speeds (read by the neighbouring
+//        slots of the same warp); after the limiter the slot is reused for
+//        the five per-cell contribution products of the slice (see S3)
+//   B2   per interface slot: amdq, apdq and Roe averages from the normal
+//        solve; overwritten by the same thread with what the cell to the left
+//        of the interface needs (dtdx*amdq, fadd, dtdx/2*B^-A^-dq, dtdx/2*B^+A^-dq)
 template <class RP, int TX, int TY, int NT, bool SPLIT> struct TileSmem {
-    static constexpr int MEQN = RP::MEQN, MW = RP::MW;
+    static constexpr int MEQN = RP::MEQN, MW = RP::MW, NROE = RP::NROE;
     static constexpr int QROWS = SPLIT ? TY + 4 : TY;
-    static constexpr int IFSZ = CMax<MW * MEQN + MW, 4 * MEQN>::value;
+    static constexpr int WBSZ = CMax<MW * MEQN + MW, 5 * MEQN>::value;
+    static constexpr int B2SZ = CMax<2 * MEQN + NROE, 4 * MEQN>::value;
     static constexpr int QX = MEQN * QROWS * TX;
-    static constexpr int total = QX + IFSZ * NT + NT;      // + reduction scratch
+    static constexpr int total = QX + (WBSZ + B2SZ) * NT + NT;      // + reduction scratch
     static constexpr int bytes = total * 8;
 };
 
 // ---------------------------------------------------------------------------
-// One chunk of one sweep direction.  IXY = 1: lines are x slices (rows), the
+// One chunk of one sweep direction: LPC = NT/32 slice lines, one warp per
+// line, one interface per lane.  IXY = 1: lines are x slices (rows) and the
 // interface index runs along x; IXY = 2: lines are y slices (columns).
 //   line : slice index (0-based; row for IXY=1, column for IXY=2)
 //   k    : interface between cells k-1 and k along the slice
-// Mode: SPLIT = dimensional splitting (no transverse terms, one update pass).
+// Lines first..first+nlines-1 are processed in chunks in increasing order.
+// S1 (normal solve) -> warp barrier -> S2 (limiter, corrections, transverse
+// solves) -> warp barrier -> S3 (per-cell contributions of the slice) ->
+// block barrier -> S4 (combine the contributions of slices line-1, line,
+// line+1 into each cell, in the reference's order) -> block barrier.
+// SPLIT = dimensional splitting (no transverse terms; each cell gets exactly
+// one contribution per sweep, so S4 is skipped).
 // ---------------------------------------------------------------------------
 template <class RP, int IXY, bool SPLIT, int TX, int TY, int NT, class Ctx>
-CLAW2_HD void sweep_chunk(const StepArgs& a, Ctx& ctx, const double* qin, double* Qx, double* IFB,
-                          int i0, int j0, int line, bool lineok, bool cflonly, int slot, int delta,
-                          int nslots, double dtn, double dtt, double& cflm)
+CLAW2_HD void sweep_chunk(const StepArgs& a, Ctx& ctx, const double* qin, double* Qx, double* WB, double* B2,
+                          int i0, int j0, int line, int cfirst, int clast, bool lineok, bool cflonly,
+                          double dtn, double dtt, double& cflm)
 {
     constexpr int MEQN = RP::MEQN, MW = RP::MW, MAUX = RP::MAUX, NROE = RP::NROE;
     constexpr int QROWS = SPLIT ? TY + 4 : TY;
     constexpr int QROW0 = SPLIT ? -2 : 0;      // tile row of Qx row 0, relative to j0
     constexpr int AUXN = MAUX > 0 ? MAUX : 1;
+    constexpr int NCELL = IXY == 1 ? TX : TY;  // cells of the tile along the slice
+    constexpr int NSLOT = NCELL + 3;           // interfaces needed along the slice
     const int tid = ctx.tid();
+    const int slot = tid & 31;
     const int len = IXY == 1 ? a.mx : a.my;
-    const int s0 = (IXY == 1 ? i0 : j0) - 1;   // first interface of the line
-    const int k = s0 + slot;
-    const bool ifok = lineok && slot < nslots && k <= len + 1;
-    // interfaces whose fluxes the tile uses: slots 1..nslots-2
-    const bool lim = ifok && !cflonly && slot >= 1 && slot <= nslots - 2 && k >= 0 && k <= len;
-    const bool cflok = ifok && slot >= 1 && slot <= nslots - 2 && k >= 0 && k <= len;
+    const int k = (IXY == 1 ? i0 : j0) - 1 + slot;   // this lane's interface
+    const bool ifok = lineok && slot < NSLOT && k <= len + 1;
+    // interfaces whose fluxes the tile uses: slots 1..NSLOT-2
+    const bool cflok = ifok && slot >= 1 && slot <= NSLOT - 2 && k >= 0 && k <= len;
+    const bool lim = cflok && !cflonly;
 
     auto cell_i = [&](int kk) { return IXY == 1 ? kk : line; };
     auto cell_j = [&](int kk) { return IXY == 1 ? line : kk; };
+    auto W = [&](int p, int m, int t) -> double& { return WB[(p * MEQN + m) * NT + t]; };
+    auto S = [&](int p, int t) -> double& { return WB[(MW * MEQN + p) * NT + t]; };
+    auto X = [&](int d, int t) -> double& { return B2[d * NT + t]; };
+    auto C = [&](int d, int m, int t) -> double& { return WB[(d * MEQN + m) * NT + t]; };
 
-    double wave[MW][MEQN], s[MW], amdq[MEQN], apdq[MEQN], roe[NROE];
     double dtl = dtn, dtr = dtn;
     // ---------------- S1: normal Riemann solve ----------------
     if (ifok) {
         double qL[MEQN], qR[MEQN], auxL[AUXN], auxR[AUXN];
+        double wave[MW][MEQN], s[MW], amdq[MEQN], apdq[MEQN], roe[NROE];
         const int iL = cell_i(k - 1), jL = cell_j(k - 1), iR = cell_i(k), jR = cell_j(k);
         if (SPLIT && IXY == 2 && !cflonly) {
             // y sweep of the split step reads the x-swept tile state
@@ -238,10 +259,11 @@ CLAW2_HD void sweep_chunk(const StepArgs& a, Ctx& ctx, const double* qin, double
                 qR[m] = Qx[(m * QROWS + (jR - j0 - QROW0)) * TX + (iR - i0)];
             }
         } else {
+            const long long oL = qoff(a, 0, iL, jL), oR = qoff(a, 0, iR, jR);
 #pragma unroll
             for (int m = 0; m < MEQN; m++) {
-                qL[m] = qin[qoff(a, m, iL, jL)];
-                qR[m] = qin[qoff(a, m, iR, jR)];
+                qL[m] = qin[oL + m * a.plane];
+                qR[m] = qin[oR + m * a.plane];
             }
         }
 #pragma unroll
@@ -249,79 +271,88 @@ CLAW2_HD void sweep_chunk(const StepArgs& a, Ctx& ctx, const double* qin, double
             auxL[m] = a.aux[qoff(a, m, iL, jL)];
             auxR[m] = a.aux[qoff(a, m, iR, jR)];
         }
-        if (a.capa >= 0) {
-            dtl = dtn / a.aux[qoff(a, a.capa, iL, jL)];
-            dtr = dtn / a.aux[qoff(a, a.capa, iR, jR)];
-        }
         RP::template rpn2<IXY>(qL, qR, auxL, auxR, a.prm, wave, s, amdq, apdq, roe);
 #pragma unroll
         for (int p = 0; p < MW; p++) {
 #pragma unroll
-            for (int m = 0; m < MEQN; m++) IFB[(p * MEQN + m) * NT + tid] = wave[p][m];
-            IFB[(MW * MEQN + p) * NT + tid] = s[p];
+            for (int m = 0; m < MEQN; m++) W(p, m, tid) = wave[p][m];
+            S(p, tid) = s[p];
+        }
+#pragma unroll
+        for (int m = 0; m < MEQN; m++) { X(m, tid) = amdq[m]; X(MEQN + m, tid) = apdq[m]; }
+#pragma unroll
+        for (int r = 0; r < NROE; r++) X(2 * MEQN + r, tid) = roe[r];
+        if (a.capa >= 0) {
+            dtl = dtn / a.aux[qoff(a, a.capa, iL, jL)];
+            dtr = dtn / a.aux[qoff(a, a.capa, iR, jR)];
         }
     }
-    ctx.sync();
+    ctx.syncwarp();
 
     // ---------------- S2: CFL, limiter, corrections, transverse ----------------
-    double fadd[MEQN], bmL[MEQN], bpL[MEQN], bmR[MEQN], bpR[MEQN];
+    // kept for S3: this interface's right-going parts (for the cell right of it)
+    double apdq[MEQN], fadd[MEQN], bmR[MEQN], bpR[MEQN];
 #pragma unroll
-    for (int m = 0; m < MEQN; m++) { fadd[m] = 0.0; bmL[m] = 0.0; bpL[m] = 0.0; bmR[m] = 0.0; bpR[m] = 0.0; }
+    for (int m = 0; m < MEQN; m++) { apdq[m] = 0.0; fadd[m] = 0.0; bmR[m] = 0.0; bpR[m] = 0.0; }
     if (cflok) {
 #pragma unroll
         for (int p = 0; p < MW; p++) {
-            const double c1 = dtr * s[p], c2 = -dtl * s[p];
+            const double sp = S(p, tid);
+            const double c1 = dtr * sp, c2 = -dtl * sp;
             cflm = cflm > c1 ? cflm : c1;
             cflm = cflm > c2 ? cflm : c2;
         }
     }
+    double cqxx[MEQN], amdq[MEQN];
     if (lim) {
-        double cqxx[MEQN];
+#pragma unroll
+        for (int m = 0; m < MEQN; m++) { amdq[m] = X(m, tid); apdq[m] = X(MEQN + m, tid); cqxx[m] = 0.0; }
         if (a.order == 2) {
-            if (a.limit_any) {
-#pragma unroll
-                for (int p = 0; p < MW; p++) {
-                    const int meth = a.mthlim[p];
-                    if (meth == 0) continue;
-                    double wnorm2 = 0.0;
-#pragma unroll
-                    for (int m = 0; m < MEQN; m++) wnorm2 = wnorm2 + wave[p][m] * wave[p][m];
-                    if (wnorm2 == 0.0) continue;
-                    // dotl = wave(k-1).wave(k) when s > 0, else dotr = wave(k).wave(k+1)
-                    const int nb = s[p] > 0.0 ? tid - delta : tid + delta;
-                    double dot = 0.0;
-#pragma unroll
-                    for (int m = 0; m < MEQN; m++) dot = dot + wave[p][m] * IFB[(p * MEQN + m) * NT + nb];
-                    const double phi = philim(wnorm2, dot, meth);
-#pragma unroll
-                    for (int m = 0; m < MEQN; m++) wave[p][m] = phi * wave[p][m];
-                }
-            }
             const double dtdxave = 0.5 * (dtl + dtr);
-            double f[MW];
 #pragma unroll
             for (int p = 0; p < MW; p++) {
-                const double as = fabs(s[p]);
-                f[p] = (a.fwave ? copysign(1.0, s[p]) : as) * (1.0 - as * dtdxave);
+                double wv[MEQN];
+#pragma unroll
+                for (int m = 0; m < MEQN; m++) wv[m] = W(p, m, tid);
+                const double sp = S(p, tid);
+                const int meth = a.mthlim[p];
+                if (a.limit_any && meth != 0) {
+                    double wnorm2 = 0.0;
+#pragma unroll
+                    for (int m = 0; m < MEQN; m++) wnorm2 = wnorm2 + wv[m] * wv[m];
+                    if (wnorm2 != 0.0) {
+                        // dotl = wave(k-1).wave(k) when s > 0, else dotr = wave(k).wave(k+1)
+                        const int nb = sp > 0.0 ? tid - 1 : tid + 1;
+                        double dot = 0.0;
+#pragma unroll
+                        for (int m = 0; m < MEQN; m++) dot = dot + wv[m] * W(p, m, nb);
+                        const double phi = philim(wnorm2, dot, meth);
+#pragma unroll
+                        for (int m = 0; m < MEQN; m++) wv[m] = phi * wv[m];
+                    }
+                }
+                const double as = fabs(sp);
+                const double f = (a.fwave ? copysign(1.0, sp) : as) * (1.0 - as * dtdxave);
+#pragma unroll
+                for (int m = 0; m < MEQN; m++) cqxx[m] = (p == 0) ? f * wv[m] : cqxx[m] + f * wv[m];
             }
 #pragma unroll
-            for (int m = 0; m < MEQN; m++) {
-                double c = 0.0;
-#pragma unroll
-                for (int p = 0; p < MW; p++) c = c + f[p] * wave[p][m];
-                cqxx[m] = c;
-                fadd[m] = 0.5 * c;
-            }
-        } else {
-#pragma unroll
-            for (int m = 0; m < MEQN; m++) cqxx[m] = 0.0;
+            for (int m = 0; m < MEQN; m++) fadd[m] = 0.5 * cqxx[m];
         }
+    }
+    if (lim) {
+        double bmL[MEQN], bpL[MEQN];
+#pragma unroll
+        for (int m = 0; m < MEQN; m++) { bmL[m] = 0.0; bpL[m] = 0.0; }
         if (!SPLIT && a.trans > 0) {
-            double A[MEQN], P[MEQN];
+            double roe[NROE], A[MEQN], P[MEQN];
+#pragma unroll
+            for (int r = 0; r < NROE; r++) roe[r] = X(2 * MEQN + r, tid);
+            const bool cor = a.order == 2 && a.trans == 2;
 #pragma unroll
             for (int m = 0; m < MEQN; m++) {
-                if (a.order == 2 && a.trans == 2) { A[m] = amdq[m] + cqxx[m]; P[m] = apdq[m] - cqxx[m]; }
-                else { A[m] = amdq[m]; P[m] = apdq[m]; }
+                A[m] = cor ? amdq[m] + cqxx[m] : amdq[m];
+                P[m] = cor ? apdq[m] - cqxx[m] : apdq[m];
             }
             double ax1[AUXN], ax2[AUXN], ax3[AUXN];
             // ilr = 1: the left-going fluctuation sits in cell k-1
@@ -347,43 +378,22 @@ CLAW2_HD void sweep_chunk(const StepArgs& a, Ctx& ctx, const double* qin, double
                 RP::template rpt2<IXY>(2, P, roe, ax1, ax2, ax3, a.prm, bmR, bpR);
             }
         }
-    }
-    ctx.sync();
-    // ---------------- S2b: publish what the cell left of the interface needs -------
-    if (lim) {
+        // publish what the cell left of the interface needs (own slot only)
         const double hl = 0.5 * dtl;
 #pragma unroll
         for (int m = 0; m < MEQN; m++) {
-            IFB[(0 * MEQN + m) * NT + tid] = dtl * amdq[m];
-            IFB[(1 * MEQN + m) * NT + tid] = fadd[m];
-            IFB[(2 * MEQN + m) * NT + tid] = hl * bmL[m];
-            IFB[(3 * MEQN + m) * NT + tid] = hl * bpL[m];
+            X(0 * MEQN + m, tid) = dtl * amdq[m];
+            X(1 * MEQN + m, tid) = fadd[m];
+            X(2 * MEQN + m, tid) = hl * bmL[m];
+            X(3 * MEQN + m, tid) = hl * bpL[m];
         }
     }
-    ctx.sync();
+    ctx.syncwarp();     // neighbours' waves and B2 slots are complete
 
-    // ---------------- S3: per-cell increments, applied in reference order --------
-    // this thread's cell is k (right of its interface); slots 1..nslots-3
-    const int ncell = (IXY == 1 ? TX : TY);
-    const bool cellok = lim && slot <= ncell && k < len;
-    double qadd[MEQN], dF[MEQN], g1[MEQN], g2[MEQN];
-    if (cellok) {
-        const double hr = 0.5 * dtr;
-        const int nb = tid + delta;
-#pragma unroll
-        for (int m = 0; m < MEQN; m++) {
-            qadd[m] = (0.0 - dtr * apdq[m]) - IFB[(0 * MEQN + m) * NT + nb];
-            dF[m] = IFB[(1 * MEQN + m) * NT + nb] - fadd[m];
-            g1[m] = (0.0 - IFB[(2 * MEQN + m) * NT + nb]) - hr * bmR[m];
-            g2[m] = (0.0 - IFB[(3 * MEQN + m) * NT + nb]) - hr * bpR[m];
-        }
-    }
+    // ---------------- S3: the slice's contributions to its cells ----------------
+    // this lane's cell is k (right of its interface); lanes 1..NCELL
+    const bool cellok = lim && slot <= NCELL && k < len;
     const bool trans = !SPLIT && a.trans > 0;
-    // tile-cell test for a cell (kk along the slice, ll = line)
-    auto in_tile = [&](int kk, int ll) {
-        const int ci = IXY == 1 ? kk : ll, cj = IXY == 1 ? ll : kk;
-        return ci >= i0 && ci < i0 + TX && ci < a.mx && cj >= j0 + QROW0 && cj < j0 + QROW0 + QROWS && cj < a.my + (SPLIT ? 2 : 0);
-    };
     auto qx = [&](int m, int kk, int ll) -> double& {
         const int ci = IXY == 1 ? kk : ll, cj = IXY == 1 ? ll : kk;
         return Qx[(m * QROWS + (cj - j0 - QROW0)) * TX + (ci - i0)];
@@ -391,76 +401,127 @@ CLAW2_HD void sweep_chunk(const StepArgs& a, Ctx& ctx, const double* qin, double
     auto capa_of = [&](int kk, int ll) {
         return a.aux[qoff(a, a.capa, IXY == 1 ? kk : ll, IXY == 1 ? ll : kk)];
     };
-    if (SPLIT) {
-        if (cellok && in_tile(k, line)) {
+    auto in_tile_line = [&](int ll) {
+        // is slice line ll a row/column of cells whose final value this tile owns?
+        return IXY == 1 ? (ll >= j0 + QROW0 && ll < j0 + QROW0 + QROWS && ll < a.my + (SPLIT ? 2 : 0))
+                        : (ll >= i0 && ll < i0 + TX && ll < a.mx);
+    };
+    if (cellok) {
+        const double hr = 0.5 * dtr;
+        const int nb = tid + 1;
+        double qadd[MEQN], dF[MEQN], g1[MEQN], g2[MEQN];
+#pragma unroll
+        for (int m = 0; m < MEQN; m++) {
+            qadd[m] = (0.0 - dtr * apdq[m]) - X(0 * MEQN + m, nb);
+            dF[m] = X(1 * MEQN + m, nb) - fadd[m];
+            g1[m] = (0.0 - X(2 * MEQN + m, nb)) - hr * bmR[m];
+            g2[m] = (0.0 - X(3 * MEQN + m, nb)) - hr * bpR[m];
+        }
+        if (SPLIT) {
+            if (in_tile_line(line)) {
+#pragma unroll
+                for (int m = 0; m < MEQN; m++) {
+                    const double q0 = IXY == 1 ? qin[qoff(a, m, k, line)] : qx(m, k, line);
+                    if (a.capa < 0) qx(m, k, line) = q0 + qadd[m] - dtn * dF[m];
+                    else qx(m, k, line) = q0 + qadd[m] - dtn * dF[m] / capa_of(k, line);
+                }
+            }
+        } else {
+            // contribution products: 0 up = dtt*g2 (to line+1), 1 qadd, 2 dtn*dF,
+            // 3 dtt*(g2-g1) (own cell), 4 dn = dtt*g1 (to line-1)
 #pragma unroll
             for (int m = 0; m < MEQN; m++) {
-                const double q0 = IXY == 1 ? qin[qoff(a, m, k, line)] : qx(m, k, line);
-                if (a.capa < 0) qx(m, k, line) = q0 + qadd[m] - dtn * dF[m];
-                else qx(m, k, line) = q0 + qadd[m] - dtn * dF[m] / capa_of(k, line);
-            }
-        }
-        ctx.sync();
-        return;
-    }
-    // pass a: contribution of this slice to the slice above (first for x: initialise)
-    if (cellok && in_tile(k, line + 1)) {
-#pragma unroll
-        for (int m = 0; m < MEQN; m++) {
-            const double q0 = IXY == 1 ? qin[qoff(a, m, k, line + 1)] : qx(m, k, line + 1);
-            if (!trans) qx(m, k, line + 1) = q0;
-            else if (a.capa < 0) qx(m, k, line + 1) = q0 + dtt * g2[m];
-            else qx(m, k, line + 1) = q0 + dtt * g2[m] / capa_of(k, line + 1);
-        }
-    }
-    ctx.sync();
-    // pass b: the slice's own cells
-    if (cellok && in_tile(k, line)) {
-#pragma unroll
-        for (int m = 0; m < MEQN; m++) {
-            double& q = qx(m, k, line);
-            if (a.capa >= 0) {
-                const double tt = trans ? dtt * (g2[m] - g1[m]) : 0.0;
-                q = q + qadd[m] - (dtn * dF[m] + tt) / capa_of(k, line);
-            } else if (IXY == 1) {
-                q = q + qadd[m] - dtn * dF[m];
-                if (trans) q = q - dtt * (g2[m] - g1[m]);
-            } else {
-                q = q + (trans ? (qadd[m] - dtn * dF[m] - dtt * (g2[m] - g1[m])) : (qadd[m] - dtn * dF[m]));
+                C(0, m, tid) = dtt * g2[m];
+                C(1, m, tid) = qadd[m];
+                C(2, m, tid) = dtn * dF[m];
+                C(3, m, tid) = dtt * (g2[m] - g1[m]);
+                C(4, m, tid) = dtt * g1[m];
             }
         }
     }
+    if (SPLIT) return;      // caller places the block barrier
     ctx.sync();
-    // pass c: contribution to the slice below
-    if (trans && cellok && in_tile(k, line - 1)) {
+
+    // ---------------- S4: combine slices line-1, line, line+1 per cell ------------
+    // Lines of this chunk: cfirst..clast.  A cell of line l receives, in this
+    // order: up(l-1), main(l), dn(l+1).  Contributions from a slice outside
+    // the chunk were applied (up) or will be applied (dn) by that chunk.
+    if (cellok) {
+        auto from = [&](int d, int m, int dw) -> double { return C(d, m, tid + 32 * dw); };
+        // (a) this line's own cells
+        if (in_tile_line(line)) {
 #pragma unroll
-        for (int m = 0; m < MEQN; m++) {
-            double& q = qx(m, k, line - 1);
-            if (a.capa < 0) q = q - dtt * g1[m];
-            else q = q - dtt * g1[m] / capa_of(k, line - 1);
+            for (int m = 0; m < MEQN; m++) {
+                double v;
+                if (line == cfirst) v = qx(m, k, line);                 // has up(line-1) already
+                else {
+                    // x sweep: start from q; y sweep: from the x-swept value
+                    v = IXY == 1 ? qin[qoff(a, m, k, line)] : qx(m, k, line);
+                    if (trans) {
+                        if (a.capa < 0) v = v + from(0, m, -1);
+                        else v = v + from(0, m, -1) / capa_of(k, line);
+                    }
+                }
+                if (a.capa >= 0) {
+                    const double tt = trans ? from(3, m, 0) : 0.0;
+                    v = v + from(1, m, 0) - (from(2, m, 0) + tt) / capa_of(k, line);
+                } else if (IXY == 1) {
+                    v = v + from(1, m, 0) - from(2, m, 0);
+                    if (trans) v = v - from(3, m, 0);
+                } else {
+                    v = v + (trans ? (from(1, m, 0) - from(2, m, 0) - from(3, m, 0)) : (from(1, m, 0) - from(2, m, 0)));
+                }
+                if (trans && line != clast) {
+                    if (a.capa < 0) v = v - from(4, m, 1);
+                    else v = v - from(4, m, 1) / capa_of(k, line);
+                }
+                qx(m, k, line) = v;
+            }
+        }
+        // (b) first contribution to the line after the chunk
+        if (line == clast && in_tile_line(line + 1)) {
+#pragma unroll
+            for (int m = 0; m < MEQN; m++) {
+                double v = IXY == 1 ? qin[qoff(a, m, k, line + 1)] : qx(m, k, line + 1);
+                if (trans) {
+                    if (a.capa < 0) v = v + from(0, m, 0);
+                    else v = v + from(0, m, 0) / capa_of(k, line + 1);
+                }
+                qx(m, k, line + 1) = v;
+            }
+        }
+        // (c) last contribution to the line before the chunk
+        if (trans && line == cfirst && in_tile_line(line - 1)) {
+#pragma unroll
+            for (int m = 0; m < MEQN; m++) {
+                double& q = qx(m, k, line - 1);
+                if (a.capa < 0) q = q - from(4, m, 0);
+                else q = q - from(4, m, 0) / capa_of(k, line - 1);
+            }
         }
     }
     ctx.sync();
 }
 
 // ---------------------------------------------------------------------------
-// Whole-tile step.  Lines per chunk LPC = NT/32; a line holds up to 32
-// interfaces (TX+3 <= 32 and TY+3 <= 32).
+// Whole-tile step: x sweeps then y sweeps, LPC = NT/32 lines per chunk.
 // ---------------------------------------------------------------------------
 template <class RP, int TX, int TY, int NT, bool SPLIT, class Ctx>
 CLAW2_HD void step_tile(const StepArgs& a, Ctx& ctx)
 {
     constexpr int MEQN = RP::MEQN;
-    constexpr int SW = 32, LPC = NT / SW;
-    static_assert(NT % SW == 0, "NT must be a multiple of 32");
-    static_assert(TX + 3 <= SW && TY + 3 <= SW, "tile too wide for one 32-slot line");
+    constexpr int LPC = NT / 32;
+    static_assert(NT % 32 == 0, "NT must be a multiple of 32");
+    static_assert(TX + 3 <= 32 && TY + 3 <= 32, "tile too wide for one 32-lane line");
     using SM = TileSmem<RP, TX, TY, NT, SPLIT>;
     constexpr int QROWS = SM::QROWS;
     constexpr int QROW0 = SPLIT ? -2 : 0;
     double* Qx = ctx.smem();
-    double* IFB = Qx + SM::QX;
-    double* red = IFB + SM::IFSZ * NT;
+    double* WB = Qx + SM::QX;
+    double* B2 = WB + SM::WBSZ * NT;
+    double* red = B2 + SM::B2SZ * NT;
     const int tid = ctx.tid();
+    const int warp = tid >> 5;
     const int i0 = ctx.bx() * TX, j0 = ctx.by() * TY;
 
     const double* qin = a.qin;
@@ -480,36 +541,46 @@ CLAW2_HD void step_tile(const StepArgs& a, Ctx& ctx)
     {
         const int nlines = SPLIT ? TY + 4 : TY + 2;
         const int first = SPLIT ? j0 - 2 : j0 - 1;
-        const int lo = SPLIT ? -2 : -1, hi = SPLIT ? a.my + 1 : a.my;
-        for (int c0 = 0; c0 < nlines; c0 += LPC) {
-            const int li = tid / SW, slot = tid % SW;
-            const int line = first + c0 + li;
-            const bool lineok = (c0 + li < nlines) && line >= lo && line <= hi;
-            sweep_chunk<RP, 1, SPLIT, TX, TY, NT>(a, ctx, qin, Qx, IFB, i0, j0, line, lineok, false,
-                                                  slot, 1, TX + 3, dtdx, dtdy, cflm);
+        const int hi = SPLIT ? a.my + 1 : a.my;
+        const int last = (first + nlines - 1 < hi) ? first + nlines - 1 : hi;
+        for (int c0 = first; c0 <= last; c0 += LPC) {
+            const int line = c0 + warp;
+            const int clast = (c0 + LPC - 1 < last) ? c0 + LPC - 1 : last;
+            sweep_chunk<RP, 1, SPLIT, TX, TY, NT>(a, ctx, qin, Qx, WB, B2, i0, j0, line, c0, clast,
+                                                  line <= last, false, dtdx, dtdy, cflm);
+            if (SPLIT) ctx.sync();
         }
     }
     // ---- y sweeps: unsplit columns i0-1..i0+TX (cols -1..mx); split the tile's
     //      columns, plus ghost columns -2,-1 / mx,mx+1 (CFL only, step2ds.f90:177)
     {
         const bool left = i0 == 0, right = i0 + TX >= a.mx;
-        const int ninner = SPLIT ? (a.mx - i0 < TX ? a.mx - i0 : TX) : TX + 2;
-        const int nlines = SPLIT ? ninner + (left ? 2 : 0) + (right ? 2 : 0) : TX + 2;
-        for (int c0 = 0; c0 < nlines; c0 += LPC) {
-            const int li = tid % LPC, slot = tid / LPC;
-            const int l = c0 + li;
-            int line;
-            bool cflonly = false;
-            if (!SPLIT) line = i0 - 1 + l;
-            else if (left && l < 2) { line = l - 2; cflonly = true; }
-            else {
-                const int r = l - (left ? 2 : 0);
-                if (r < ninner) line = i0 + r;
-                else { line = a.mx + (r - ninner); cflonly = true; }
+        const int ninner = SPLIT ? (a.mx - i0 < TX ? a.mx - i0 : TX) : 0;
+        if (!SPLIT) {
+            const int first = i0 - 1;
+            const int last = (i0 + TX < a.mx) ? i0 + TX : a.mx;
+            for (int c0 = first; c0 <= last; c0 += LPC) {
+                const int line = c0 + warp;
+                const int clast = (c0 + LPC - 1 < last) ? c0 + LPC - 1 : last;
+                sweep_chunk<RP, 2, SPLIT, TX, TY, NT>(a, ctx, qin, Qx, WB, B2, i0, j0, line, c0, clast,
+                                                      line <= last, false, dtdy, dtdx, cflm);
             }
-            const bool lineok = l < nlines && line >= (SPLIT ? -2 : -1) && line <= (SPLIT ? a.mx + 1 : a.mx);
-            sweep_chunk<RP, 2, SPLIT, TX, TY, NT>(a, ctx, qin, Qx, IFB, i0, j0, line, lineok, cflonly,
-                                                  slot, LPC, TY + 3, dtdy, dtdx, cflm);
+        } else {
+            const int nlines = ninner + (left ? 2 : 0) + (right ? 2 : 0);
+            for (int c0 = 0; c0 < nlines; c0 += LPC) {
+                const int l = c0 + warp;
+                int line;
+                bool cflonly = false;
+                if (left && l < 2) { line = l - 2; cflonly = true; }
+                else {
+                    const int r = l - (left ? 2 : 0);
+                    if (r < ninner) line = i0 + r;
+                    else { line = a.mx + (r - ninner); cflonly = true; }
+                }
+                sweep_chunk<RP, 2, SPLIT, TX, TY, NT>(a, ctx, qin, Qx, WB, B2, i0, j0, line, 0, 0,
+                                                      l < nlines, cflonly, dtdy, dtdx, cflm);
+                ctx.sync();
+            }
         }
     }
 

@@ -94,7 +94,9 @@ template <bool TRACER> struct RpEuler {
         // entropy fix, :205-286
         {
             const double rhoim1 = qL[0];
-            const double pim1 = gamma1 * (qL[3] - 0.5 * (qL[mu] * qL[mu] + qL[mv] * qL[mv]) / rhoim1);
+            // gamma1*(qr(4,i-1) - 0.5*(qr(mu,i-1)**2 + qr(mv,i-1)**2)/rhoim1) is pl bit for bit:
+            // the two squares are the same and IEEE addition commutes
+            const double pim1 = pl;
             const double cim1 = sqrt(gamma * pim1 / rhoim1);
             const double s0 = qL[mu] / rhoim1 - cim1;
             if (s0 >= 0.0 && s[0] > 0.0) {
@@ -125,7 +127,7 @@ template <bool TRACER> struct RpEuler {
                     amdq[3] = amdq[3] + s[2] * wave[2][3];
                     if constexpr (TRACER) amdq[4] = amdq[4] + s[4] * wave[4][4];
                     const double rhoi = qR[0];
-                    const double pi = gamma1 * (qR[3] - 0.5 * (qR[mu] * qR[mu] + qR[mv] * qR[mv]) / rhoi);
+                    const double pi = pr;   // same value as pr, see pim1
                     const double ci = sqrt(gamma * pi / rhoi);
                     const double s3 = qR[mu] / rhoi + ci;
                     const double rho2 = qR[0] - wave[3][0];

@@ -67,6 +67,11 @@ class DeviceState(object):
     def host_q_touched(self):
         self.host_dirty = True
 
+    def host_q_assigned(self):
+        """state.q was replaced on the host: the host copy is now authoritative."""
+        self.host_dirty = True
+        self.device_newer = False
+
     def host_aux_touched(self):
         self.aux_dirty = True
 

@@ -43,7 +43,7 @@ class State(object):
     def q(self, value):
         self._q = value
         if self._dev is not None:
-            self._dev.host_q_touched()
+            self._dev.host_q_assigned()
 
     @property
     def aux(self):
