@@ -173,6 +173,26 @@ CLAW2_EXPORT int claw2_step(const claw2_problem* p, const double* q_in, double* 
                const double* aux, double dt, void* scratch, double* cfl_dev,
                void* stream);
 
+/* Largest number of tiles (29x29 cells each, 28x28 with dimensional
+ * splitting) that claw2_step_noalloc accepts: ceil(mx/29)*ceil(my/29) <= 32768,
+ * i.e. about 27 million cells. */
+#define CLAW2_NOALLOC_MAX_TILES 32768
+
+/* claw2_step without any device allocation, for callers that may not allocate
+ * GPU memory (their memory belongs to a pool they manage, their time loop must
+ * not call the allocator, or their language binding cannot own device memory).
+ * No counterpart in the reference.  Same arguments and results as claw2_step
+ * minus `scratch`: the scratch is a static array inside this library
+ * (64 + 8*CLAW2_NOALLOC_MAX_TILES bytes, held by every GPU that loads the
+ * library until the process exits).  The first call on a device looks up that
+ * array's address for the current device; make that first call before any
+ * stream capture begins.  Problems with more tiles than the maximum return
+ * CLAW2_ERR_SIZE.  All calls share the one array, so calls that overlap on the
+ * GPU (different streams, or different host threads, on the same device) race;
+ * order them on one stream. */
+CLAW2_EXPORT int claw2_step_noalloc(const claw2_problem* p, const double* q_in, double* q_out,
+                                    const double* aux, double dt, double* cfl_dev, void* stream);
+
 /* Launch nsteps controlled steps.  q0/q1 are the two state buffers; ctrl->cur
  * says which holds the current state.  Each launch reads dt from ctrl, steps
  * q[cur] -> q[1-cur] and updates ctrl exactly as one iteration of

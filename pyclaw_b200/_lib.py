@@ -30,6 +30,7 @@ PROTOTYPES = [
     ("claw2_fill_ghosts", ctypes.c_int, [_P, _dp, _vp]),
     ("claw2_fill_aux_ghosts", ctypes.c_int, [_P, _dp, _vp]),
     ("claw2_step", ctypes.c_int, [_P, _dp, _dp, _dp, _dbl, _vp, _dp, _vp]),
+    ("claw2_step_noalloc", ctypes.c_int, [_P, _dp, _dp, _dp, _dbl, _dp, _vp]),
     ("claw2_advance", ctypes.c_int, [_P, _dp, _dp, _dp, _vp, _vp, ctypes.c_int, _vp]),
     ("claw2_control_init", ctypes.c_int, [_C, _dbl, _dbl, _dbl, _dbl, _dbl, _dbl, ctypes.c_int,
                                           ctypes.c_int, _i64, _dbl]),

@@ -4,6 +4,7 @@
 // reproduces the reference's operation-by-operation rounding).
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cmath>
 #include <cstdint>
 #include <cstdlib>
@@ -453,6 +454,49 @@ int claw2_device_to_ref(const claw2_problem* p, int ncomp, const double* dev, do
 {
     if (!p || !ref || !dev || ncomp < 1) return CLAW2_ERR_INVALID;
     return conv(p, ncomp, dev, ref, false, true, S(stream));
+}
+
+// ---------------------------------------------------------------------------
+// allocation-free step
+//
+// Some callers cannot allocate GPU memory: a host code that hands all device
+// memory to its own pool at start-up, a time loop that must not enter the CUDA
+// allocator (an allocation can synchronise the device), or a foreign-language
+// binding that can pass pointers to existing buffers but cannot own device
+// allocations.  claw2_step_noalloc serves them: its scratch (the block-arrival
+// counter and one CFL partial per tile) is the static array below, which every
+// GPU that loads this library holds until the process exits.
+// ---------------------------------------------------------------------------
+static __device__ __align__(256) unsigned char g_noalloc_scratch[64 + 8 * CLAW2_NOALLOC_MAX_TILES];
+
+namespace {
+constexpr int kMaxDevices = 64;
+std::atomic<void*> g_noalloc_addr[kMaxDevices];   // device address of g_noalloc_scratch, per device
+}
+
+int claw2_step_noalloc(const claw2_problem* p, const double* q_in, double* q_out, const double* aux, double dt,
+                       double* cfl_dev, void* stream)
+{
+    int rc = claw2_validate(p);
+    if (rc) return rc;
+    if (!q_in || !q_out || !cfl_dev || (p->num_aux > 0 && !aux) || q_in == q_out) return CLAW2_ERR_INVALID;
+    int nbx, nby;
+    tiles(p, &nbx, &nby);
+    if ((long long)nbx * (long long)nby > CLAW2_NOALLOC_MAX_TILES) return CLAW2_ERR_SIZE;
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess) return CLAW2_ERR_CUDA;
+    if (dev < 0 || dev >= kMaxDevices) return CLAW2_ERR_UNSUPPORTED;
+    // Set-up, once per device, with that device current: the name of a
+    // __device__ variable is only a host-side stand-in, so the kernel gets the
+    // address the runtime reports for this device.
+    void* scratch = g_noalloc_addr[dev].load(std::memory_order_acquire);
+    if (!scratch) {
+        if (cudaGetSymbolAddress(&scratch, g_noalloc_scratch) != cudaSuccess || !scratch) return CLAW2_ERR_CUDA;
+        g_noalloc_addr[dev].store(scratch, std::memory_order_release);
+    }
+    // the array keeps the previous call's contents; the arrival counter must start at zero
+    if (cudaMemsetAsync(scratch, 0, 64, S(stream)) != cudaSuccess) return CLAW2_ERR_CUDA;
+    return claw2_step(p, q_in, q_out, aux, dt, scratch, cfl_dev, stream);
 }
 
 // ---------------------------------------------------------------------------
