@@ -367,11 +367,12 @@ def run_ours(args, world, rank, local):
     avg_kernel_s = t_dev / args.steps
     achieved = alg_bytes / avg_kernel_s / 1e9
     traffic = None
-    tpath = os.path.join(ROOT, "profiles", "step_kernel_traffic.json")
-    if os.path.exists(tpath):
+    tpath = os.path.join(ROOT, "profiles", "step_kernel_euler1280x320.md")
+    if os.path.exists(tpath):            # dram read+write bytes of one launch, from the ncu capture
         with open(tpath) as f:
-            tj = json.load(f)
-        traffic = tj.get("dram_bytes_per_launch_scaled")
+            for ln in f:
+                if ln.startswith("traffic_bytes_per_launch:"):
+                    traffic = int(ln.split(":")[1])
 
     # ---- e2e through the host-buffer C ABI (claw2_session_evolve) ----------
     e2e = None
