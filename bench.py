@@ -104,6 +104,41 @@ def acoustics_config(n=256):
     return prob, q, None, run, 0.6
 
 
+def batched_vc_config(n=1024, seed=2024, nmin=64, nmax=384):
+    """1024 variable-coefficient acoustics instances: nx, ny ~ U{64..384}; aux
+    (rho, c=sqrt(K/rho)) piecewise constant over U{2..6} vertical layers with
+    rho, K ~ U[1,4]; Gaussian pressure pulse of width 0.05 at a random interior
+    point; MC, unsplit with transverse_waves=2, walls at the lower and
+    extrapolation at the upper boundaries.  Returns (problem, instances)."""
+    from pyclaw_b200 import _abi
+    rng = np.random.default_rng(seed)
+    insts = []
+    for _ in range(n):
+        nx, ny = (int(v) for v in rng.integers(nmin, nmax + 1, size=2))
+        nl = int(rng.integers(2, 7))
+        xs = np.sort(rng.uniform(0.0, 1.0, nl - 1))
+        rho = rng.uniform(1.0, 4.0, nl)
+        K = rng.uniform(1.0, 4.0, nl)
+        c = np.sqrt(K / rho)
+        x, dx = _centers(0.0, 1.0, nx)
+        y, dy = _centers(0.0, 1.0, ny)
+        X, Y = np.meshgrid(x, y, indexing='ij')
+        layer = np.searchsorted(xs, x)
+        aux = np.empty((2, nx, ny), order='F')
+        aux[0] = rho[layer][:, None]
+        aux[1] = c[layer][:, None]
+        x0, y0 = rng.uniform(0.1, 0.9, size=2)
+        q = np.zeros((3, nx, ny), order='F')
+        q[0] = np.exp(-((X - x0) ** 2 + (Y - y0) ** 2) / 0.05 ** 2)
+        insts.append(dict(q=q, aux=aux, dx=dx, dy=dy, dt=0.9 * min(dx, dy) / float(c.max())))
+    prob = _abi.make_problem(rp=_abi.RP_VC_ACOUSTICS, num_eqn=3, num_waves=2, num_aux=2, mx=64, my=64,
+                             dx=1.0, dy=1.0, order=2, transverse=2, mthlim=[4],
+                             bc_lower=(_abi.BC_WALL, _abi.BC_WALL), bc_upper=(_abi.BC_EXTRAP, _abi.BC_EXTRAP),
+                             aux_bc_lower=(_abi.BC_WALL, _abi.BC_WALL),
+                             aux_bc_upper=(_abi.BC_EXTRAP, _abi.BC_EXTRAP))
+    return prob, insts
+
+
 def make_solver(pc, prob, run):
     """A ClawSolver2D configured like `prob` (Euler shock-bubble settings)."""
     solver = pc.ClawSolver2D(pc.riemann.rp2_euler_4wave)

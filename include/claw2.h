@@ -216,6 +216,48 @@ CLAW2_EXPORT int claw2_ref_to_device(const claw2_problem* p, int ncomp, const do
 CLAW2_EXPORT int claw2_device_to_ref(const claw2_problem* p, int ncomp, const double* dev,
                         double* ref, void* stream);
 
+/* ---- batched form: many independent instances per launch --------------- */
+/* One instance of a batch: its own grid size, spacing, state buffers (device
+ * layout of that grid), aux, controller and scratch.  All instances share the
+ * solver settings of the claw2_problem passed with them (Riemann solver,
+ * limiters, order, transverse mode, boundary conditions); its mx, my, dx, dy
+ * are ignored.  No counterpart in the reference, which steps one patch per
+ * call. */
+typedef struct claw2_batch_instance {
+    double* q0;                 /* state buffers (device layout for this grid) */
+    double* q1;
+    const double* aux;          /* may be NULL when num_aux == 0               */
+    claw2_control* ctrl;        /* this instance's time-step controller        */
+    double* partials;           /* one double per tile of this instance        */
+    unsigned int* ticket;       /* arrival counter, zero between launches      */
+    int64_t ld, plane;          /* layout of this grid (claw2_get_layout)      */
+    int32_t mx, my;
+    double dx, dy;
+    int32_t nbx, nby;           /* tiles (claw2_batch_tiles)                   */
+    int32_t tile_begin;         /* index of this instance's first tile         */
+    int32_t pad_;
+} claw2_batch_instance;
+
+/* Launch configurations of the batched kernel the autotuner chooses from. */
+CLAW2_EXPORT int claw2_batch_num_variants(void);
+/* Threads per CTA and resident CTAs per SM of variant v (for reporting). */
+CLAW2_EXPORT int claw2_batch_variant_info(int v, int* threads, int* ctas_per_sm);
+/* Tiles of an mx x my instance. */
+CLAW2_EXPORT int claw2_batch_tiles(int mx, int my, int* nbx, int* nby);
+/* nsteps launches of the batched step: every launch takes one controlled step
+ * (Solver.evolve_to_time's loop body, src/pyclaw/solver.py:632-691) of every
+ * instance whose controller is not done, each with its own dt.  inst is a
+ * device array of ninst descriptors whose tiles are numbered consecutively;
+ * ntiles is their total.  Unsplit (transverse >= 0) only. */
+CLAW2_EXPORT int claw2_batch_advance(const claw2_problem* p, const claw2_batch_instance* inst, int ninst,
+                                     int ntiles, int nsteps, int variant, void* stream);
+/* The same nsteps launches captured once into a CUDA graph; replay it with
+ * claw2_graph_launch.  The descriptors and buffers must stay where they are. */
+CLAW2_EXPORT int claw2_batch_graph_create(const claw2_problem* p, const claw2_batch_instance* inst, int ninst,
+                                          int ntiles, int nsteps, int variant, void** graph_exec);
+CLAW2_EXPORT int claw2_graph_launch(void* graph_exec, void* stream);
+CLAW2_EXPORT int claw2_graph_destroy(void* graph_exec);
+
 /* ---- host-buffer session (reference layout, host pointers) ----------- */
 /* A session owns device buffers for one problem so that callers holding host
  * arrays (the f2py calling convention of step2) can step without managing

@@ -36,6 +36,16 @@ PROTOTYPES = [
                                           ctypes.c_int, _i64, _dbl]),
     ("claw2_ref_to_device", ctypes.c_int, [_P, ctypes.c_int, _dp, _dp, _vp]),
     ("claw2_device_to_ref", ctypes.c_int, [_P, ctypes.c_int, _dp, _dp, _vp]),
+    ("claw2_batch_num_variants", ctypes.c_int, []),
+    ("claw2_batch_variant_info", ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                                ctypes.POINTER(ctypes.c_int)]),
+    ("claw2_batch_tiles", ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                         ctypes.POINTER(ctypes.c_int)]),
+    ("claw2_batch_advance", ctypes.c_int, [_P, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp]),
+    ("claw2_batch_graph_create", ctypes.c_int, [_P, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                                ctypes.POINTER(_vp)]),
+    ("claw2_graph_launch", ctypes.c_int, [_vp, _vp]),
+    ("claw2_graph_destroy", ctypes.c_int, [_vp]),
     ("claw2_session_create", ctypes.c_int, [_P, ctypes.POINTER(_vp)]),
     ("claw2_session_destroy", ctypes.c_int, [_vp]),
     ("claw2_session_step2", ctypes.c_int, [_vp, _dp, _dp, _dp, _dbl, ctypes.POINTER(_dbl)]),

@@ -48,6 +48,34 @@ __global__ void __launch_bounds__(NT, CLAW2_MINB) step_kernel(StepArgs a)
     step_tile<RP, TX, TY, NT, SPLIT>(a, ctx);
 }
 
+// Batched step: a persistent grid walks the concatenated tile list of all
+// instances; each tile is one step_tile_at call with that instance's buffers.
+template <class RP, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB)
+batch_kernel(const claw2_batch_instance* __restrict__ inst, int ninst, int ntiles, StepArgs common)
+{
+    extern __shared__ double smem_dyn[];
+    DevCtx ctx{smem_dyn};
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        int lo = 0, hi = ninst - 1;                 // last instance with tile_begin <= t
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (inst[mid].tile_begin <= t) lo = mid;
+            else hi = mid - 1;
+        }
+        const claw2_batch_instance& I = inst[lo];
+        StepArgs a = common;
+        a.q0 = I.q0; a.q1 = I.q1; a.aux = I.aux; a.ctrl = I.ctrl;
+        a.partials = I.partials; a.ticket = I.ticket;
+        a.ld = I.ld; a.plane = I.plane; a.mx = I.mx; a.my = I.my; a.dx = I.dx; a.dy = I.dy;
+        a.ghost_fused = (I.mx >= 4 && I.my >= 4) ? common.ghost_fused : 0;
+        const int lt = t - I.tile_begin;
+        const TileId tile{lt % I.nbx, lt / I.nbx, I.nbx, I.nby, lt, I.nbx * I.nby};
+        step_tile_at<RP, 29, 29, NT, false>(a, ctx, tile);
+        __syncthreads();                            // shared memory is reused by the next tile
+    }
+}
+
 // Tile shapes: a line of a chunk has 32 interface slots, so TX+3, TY+3 <= 32.
 #ifndef CLAW2_UNT
 #define CLAW2_UNT 256
@@ -457,6 +485,156 @@ int claw2_device_to_ref(const claw2_problem* p, int ncomp, const double* dev, do
 }
 
 // ---------------------------------------------------------------------------
+// batched form
+// ---------------------------------------------------------------------------
+}  // extern "C"
+
+namespace {
+struct BatchVariant { int threads, minb; };
+constexpr BatchVariant kBatchVariants[] = {{256, 2}, {128, 4}, {128, 3}, {512, 1}};
+constexpr int kNumBatchVariants = sizeof(kBatchVariants) / sizeof(kBatchVariants[0]);
+
+template <class RP, int NT, int MINB>
+int batch_launch_t(const StepArgs& common, const claw2_batch_instance* inst, int ninst, int ntiles, int nsteps,
+                   cudaStream_t st)
+{
+    using SM = TileSmem<RP, 29, 29, NT, false>;
+    auto kern = batch_kernel<RP, NT, MINB>;
+    static int grid = 0;
+    if (grid == 0) {
+        if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SM::bytes) != cudaSuccess)
+            return CLAW2_ERR_CUDA;
+        int dev = 0, nsm = 0, occ = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, NT, SM::bytes) != cudaSuccess || occ < 1)
+            return CLAW2_ERR_CUDA;
+        grid = nsm * occ;
+    }
+    const int g = ntiles < grid ? ntiles : grid;
+    for (int n = 0; n < nsteps; n++) {
+        kern<<<g, NT, SM::bytes, st>>>(inst, ninst, ntiles, common);
+        if (cudaGetLastError() != cudaSuccess) return CLAW2_ERR_CUDA;
+    }
+    return CLAW2_OK;
+}
+
+template <class RP>
+int batch_launch_rp(int variant, const StepArgs& c, const claw2_batch_instance* inst, int ninst, int ntiles,
+                    int nsteps, cudaStream_t st)
+{
+    switch (variant) {
+    case 0: return batch_launch_t<RP, 256, 2>(c, inst, ninst, ntiles, nsteps, st);
+    case 1: return batch_launch_t<RP, 128, 4>(c, inst, ninst, ntiles, nsteps, st);
+    case 2: return batch_launch_t<RP, 128, 3>(c, inst, ninst, ntiles, nsteps, st);
+    case 3: return batch_launch_t<RP, 512, 1>(c, inst, ninst, ntiles, nsteps, st);
+    default: return CLAW2_ERR_INVALID;
+    }
+}
+
+int batch_launch(const claw2_problem* p, const claw2_batch_instance* inst, int ninst, int ntiles, int nsteps,
+                 int variant, cudaStream_t st)
+{
+    StepArgs c;
+    fill_args(p, nullptr, c);
+    c.ghost_fused = 1;
+    for (int d = 0; d < 2; d++)
+        if (p->bc_lower[d] == CLAW2_BC_CUSTOM || p->bc_upper[d] == CLAW2_BC_CUSTOM) return CLAW2_ERR_UNSUPPORTED;
+    switch (p->rp) {
+    case CLAW2_RP_ACOUSTICS: return batch_launch_rp<RpAcoustics>(variant, c, inst, ninst, ntiles, nsteps, st);
+    case CLAW2_RP_VC_ACOUSTICS: return batch_launch_rp<RpVcAcoustics>(variant, c, inst, ninst, ntiles, nsteps, st);
+    case CLAW2_RP_EULER_4WAVE: return batch_launch_rp<RpEuler<false>>(variant, c, inst, ninst, ntiles, nsteps, st);
+    case CLAW2_RP_EULER_5WAVE: return batch_launch_rp<RpEuler<true>>(variant, c, inst, ninst, ntiles, nsteps, st);
+    case CLAW2_RP_SHALLOW_ROE: return batch_launch_rp<RpShallow>(variant, c, inst, ninst, ntiles, nsteps, st);
+    default: return CLAW2_ERR_INVALID;
+    }
+}
+
+int batch_check(const claw2_problem* p, const claw2_batch_instance* inst, int ninst, int ntiles, int nsteps,
+                int variant)
+{
+    if (!p || !inst || ninst < 1 || ntiles < 1 || nsteps < 0) return CLAW2_ERR_INVALID;
+    if (variant < 0 || variant >= kNumBatchVariants) return CLAW2_ERR_INVALID;
+    if (p->transverse < 0) return CLAW2_ERR_UNSUPPORTED;
+    int meqn, mw, maux;
+    if (solver_shape(p->rp, &meqn, &mw, &maux) || p->num_eqn != meqn || p->num_waves != mw || p->num_aux < maux)
+        return CLAW2_ERR_INVALID;
+    if (p->num_ghost != CLAW2_NUM_GHOST || p->index_capa >= p->num_aux) return CLAW2_ERR_INVALID;
+    for (int d = 0; d < 2; d++)
+        if (!periodic_ok(p->bc_lower[d], p->bc_upper[d])) return CLAW2_ERR_UNSUPPORTED;
+    return CLAW2_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int claw2_batch_num_variants(void) { return kNumBatchVariants; }
+
+int claw2_batch_variant_info(int v, int* threads, int* ctas_per_sm)
+{
+    if (v < 0 || v >= kNumBatchVariants || !threads || !ctas_per_sm) return CLAW2_ERR_INVALID;
+    *threads = kBatchVariants[v].threads;
+    *ctas_per_sm = kBatchVariants[v].minb;
+    return CLAW2_OK;
+}
+
+int claw2_batch_tiles(int mx, int my, int* nbx, int* nby)
+{
+    if (mx < 4 || my < 4 || !nbx || !nby) return CLAW2_ERR_INVALID;
+    *nbx = (mx + UTX - 1) / UTX;
+    *nby = (my + UTY - 1) / UTY;
+    return CLAW2_OK;
+}
+
+int claw2_batch_advance(const claw2_problem* p, const claw2_batch_instance* inst, int ninst, int ntiles, int nsteps,
+                        int variant, void* stream)
+{
+    int rc = batch_check(p, inst, ninst, ntiles, nsteps, variant);
+    if (rc) return rc;
+    return batch_launch(p, inst, ninst, ntiles, nsteps, variant, S(stream));
+}
+
+int claw2_batch_graph_create(const claw2_problem* p, const claw2_batch_instance* inst, int ninst, int ntiles,
+                             int nsteps, int variant, void** graph_exec)
+{
+    int rc = batch_check(p, inst, ninst, ntiles, nsteps, variant);
+    if (rc) return rc;
+    if (!graph_exec) return CLAW2_ERR_INVALID;
+    // one launch outside the capture configures the kernel (shared-memory
+    // attribute, occupancy) so that the capture itself only records launches
+    cudaStream_t st;
+    if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) return CLAW2_ERR_CUDA;
+    rc = batch_launch(p, inst, ninst, ntiles, 0, variant, st);
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    if (!rc && cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) rc = CLAW2_ERR_CUDA;
+    if (!rc) {
+        const int r2 = batch_launch(p, inst, ninst, ntiles, nsteps, variant, st);
+        if (cudaStreamEndCapture(st, &graph) != cudaSuccess || r2) rc = r2 ? r2 : CLAW2_ERR_CUDA;
+    }
+    if (!rc && cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess) rc = CLAW2_ERR_CUDA;
+    if (graph) cudaGraphDestroy(graph);
+    cudaStreamDestroy(st);
+    if (rc) return rc;
+    *graph_exec = exec;
+    return CLAW2_OK;
+}
+
+int claw2_graph_launch(void* graph_exec, void* stream)
+{
+    if (!graph_exec) return CLAW2_ERR_INVALID;
+    return cudaGraphLaunch(reinterpret_cast<cudaGraphExec_t>(graph_exec), S(stream)) == cudaSuccess ? CLAW2_OK
+                                                                                                     : CLAW2_ERR_CUDA;
+}
+
+int claw2_graph_destroy(void* graph_exec)
+{
+    if (!graph_exec) return CLAW2_OK;
+    return cudaGraphExecDestroy(reinterpret_cast<cudaGraphExec_t>(graph_exec)) == cudaSuccess ? CLAW2_OK
+                                                                                               : CLAW2_ERR_CUDA;
+}
+
+// ---------------------------------------------------------------------------
 // allocation-free step
 //
 // Some callers cannot allocate GPU memory: a host code that hands all device
@@ -467,12 +645,16 @@ int claw2_device_to_ref(const claw2_problem* p, int ncomp, const double* dev, do
 // counter and one CFL partial per tile) is the static array below, which every
 // GPU that loads this library holds until the process exits.
 // ---------------------------------------------------------------------------
+}  // extern "C"
+
 static __device__ __align__(256) unsigned char g_noalloc_scratch[64 + 8 * CLAW2_NOALLOC_MAX_TILES];
 
 namespace {
 constexpr int kMaxDevices = 64;
 std::atomic<void*> g_noalloc_addr[kMaxDevices];   // device address of g_noalloc_scratch, per device
 }
+
+extern "C" {
 
 int claw2_step_noalloc(const claw2_problem* p, const double* q_in, double* q_out, const double* aux, double dt,
                        double* cfl_dev, void* stream)

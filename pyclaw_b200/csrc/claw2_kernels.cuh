@@ -506,8 +506,15 @@ CLAW2_HD void sweep_chunk(const StepArgs& a, Ctx& ctx, const double* qin, double
 // ---------------------------------------------------------------------------
 // Whole-tile step: x sweeps then y sweeps, LPC = NT/32 lines per chunk.
 // ---------------------------------------------------------------------------
+// Tile coordinates of one CTA's work item: tile (bx, by) of an nbx x nby grid
+// of tiles; `part` is this tile's slot in a.partials and `ntiles` the number of
+// tiles that report to the same arrival counter (a.ticket).
+struct TileId {
+    int bx, by, nbx, nby, part, ntiles;
+};
+
 template <class RP, int TX, int TY, int NT, bool SPLIT, class Ctx>
-CLAW2_HD void step_tile(const StepArgs& a, Ctx& ctx)
+CLAW2_HD void step_tile_at(const StepArgs& a, Ctx& ctx, const TileId& tile)
 {
     constexpr int MEQN = RP::MEQN;
     constexpr int LPC = NT / 32;
@@ -522,7 +529,7 @@ CLAW2_HD void step_tile(const StepArgs& a, Ctx& ctx)
     double* red = B2 + SM::B2SZ * NT;
     const int tid = ctx.tid();
     const int warp = tid >> 5;
-    const int i0 = ctx.bx() * TX, j0 = ctx.by() * TY;
+    const int i0 = tile.bx * TX, j0 = tile.by * TY;
 
     const double* qin = a.qin;
     double* qout = a.qout;
@@ -609,8 +616,8 @@ CLAW2_HD void step_tile(const StepArgs& a, Ctx& ctx)
             if (red[t] < 0.0) nf = 1;
             else mxv = mxv > red[t] ? mxv : red[t];
         }
-        const int nblocks = ctx.nbx() * ctx.nby();
-        const int bid = ctx.by() * ctx.nbx() + ctx.bx();
+        const int nblocks = tile.ntiles;
+        const int bid = tile.part;
         a.partials[bid] = nf ? -1.0 : mxv;
         ctx.fence();
         const unsigned int prev = ctx.atomic_inc(a.ticket);
@@ -629,6 +636,13 @@ CLAW2_HD void step_tile(const StepArgs& a, Ctx& ctx)
             ctx.fence();
         }
     }
+}
+
+template <class RP, int TX, int TY, int NT, bool SPLIT, class Ctx>
+CLAW2_HD void step_tile(const StepArgs& a, Ctx& ctx)
+{
+    const TileId t{ctx.bx(), ctx.by(), ctx.nbx(), ctx.nby(), ctx.by() * ctx.nbx() + ctx.bx(), ctx.nbx() * ctx.nby()};
+    step_tile_at<RP, TX, TY, NT, SPLIT>(a, ctx, t);
 }
 
 }  // namespace claw2

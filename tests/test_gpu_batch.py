@@ -1,0 +1,72 @@
+"""Batched form: every instance of a batch must be bit-identical to the same
+instance stepped alone by the plain device path, whatever launch variant the
+autotuner picks, and one instance is checked against the oracle."""
+import ctypes
+
+import numpy as np
+import pytest
+
+import bench
+from pyclaw_b200 import _abi, _lib
+
+pytestmark = pytest.mark.gpu
+
+
+def _alone(prob, inst, nsteps):
+    """The instance run by itself: DeviceState + the device-controlled loop."""
+    import torch
+    from pyclaw_b200.device import DeviceState
+    pk = _abi.Problem.from_buffer_copy(prob)
+    pk.mx, pk.my = inst["q"].shape[1], inst["q"].shape[2]
+    pk.dx, pk.dy = inst["dx"], inst["dy"]
+    dev = DeviceState(pk)
+    dev.upload_aux(inst["aux"])
+    dev.upload_q(inst["q"])
+    lib = _lib.load()
+    c = _abi.Control()
+    lib.claw2_control_init(ctypes.byref(c), 0.0, inst["dt"], 1e300, 1.0, 0.9, 1e99, 1, 0, nsteps, 0.9)
+    out = dev.evolve(c)
+    torch.cuda.synchronize()
+    return dev.download_q(), out
+
+
+def test_batch_instances_equal_single_runs(orc):
+    prob, insts = bench.batched_vc_config(n=12, seed=7, nmin=20, nmax=90)
+    from pyclaw_b200.batch import BatchSolver
+    bs = BatchSolver(prob, insts)
+    bs.init_controls([i["dt"] for i in insts], max_steps=40)
+    tuning = bs.autotune(steps=2, repeats=1)
+    assert tuning["chosen"] in tuning["candidates"]
+    bs.advance_graph(45, chunk=20)           # more launches than needed: done instances idle
+    ctrls = bs.controls()
+    for k in (0, 3, 7, 11):
+        q_alone, c_alone = _alone(prob, insts[k], 40)
+        assert ctrls[k].numsteps == c_alone.numsteps and ctrls[k].t == c_alone.t and ctrls[k].dt == c_alone.dt
+        assert np.array_equal(bs.solution(k), q_alone)
+    # one instance against the oracle's replay of evolve_to_time
+    k = 5
+    pk = bs.problems[k]
+    ref = orc.Run(pk, insts[k]["q"], insts[k]["aux"], cfl_max=1.0, cfl_desired=0.9, dt_initial=insts[k]["dt"],
+                  max_steps=40)
+    try:
+        ref.evolve_to_time(1e300)
+    except Exception as e:                   # 40 iterations reached before tend, as configured
+        assert "Maximum number of timesteps" in str(e)
+    assert np.array_equal(bs.solution(k), ref.q)
+    bs.close()
+
+
+def test_batch_variants_agree():
+    prob, insts = bench.batched_vc_config(n=5, seed=3, nmin=30, nmax=70)
+    from pyclaw_b200.batch import BatchSolver
+    results = []
+    for v in range(_lib.load().claw2_batch_num_variants()):
+        bs = BatchSolver(prob, insts)
+        bs.init_controls([i["dt"] for i in insts], max_steps=10)
+        bs.variant = v
+        bs.advance(10)
+        results.append([bs.solution(k) for k in range(len(insts))])
+        bs.close()
+    for r in results[1:]:
+        for a, b in zip(results[0], r):
+            assert np.array_equal(a, b)
