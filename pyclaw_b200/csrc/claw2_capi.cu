@@ -60,7 +60,7 @@ batch_kernel(const claw2_batch_instance* __restrict__ inst, int ninst, int ntile
         int lo = 0, hi = ninst - 1;                 // last instance with tile_begin <= t
         while (lo < hi) {
             const int mid = (lo + hi + 1) >> 1;
-            if (inst[mid].tile_begin <= t) lo = mid;
+            if (__ldg(&inst[mid].tile_begin) <= t) lo = mid;
             else hi = mid - 1;
         }
         const claw2_batch_instance& I = inst[lo];

@@ -251,6 +251,8 @@ CLAW2_HD void sweep_chunk(const StepArgs& a, Ctx& ctx, const double* qin, double
         double qL[MEQN], qR[MEQN], auxL[AUXN], auxR[AUXN];
         double wave[MW][MEQN], s[MW], amdq[MEQN], apdq[MEQN], roe[NROE];
         const int iL = cell_i(k - 1), jL = cell_j(k - 1), iR = cell_i(k), jR = cell_j(k);
+        const long long oL = qoff(a, 0, iL, jL);
+        const long long oR = oL + (IXY == 1 ? 1 : a.ld);      // cell k: one step along the slice
         if (SPLIT && IXY == 2 && !cflonly) {
             // y sweep of the split step reads the x-swept tile state
 #pragma unroll
@@ -259,7 +261,6 @@ CLAW2_HD void sweep_chunk(const StepArgs& a, Ctx& ctx, const double* qin, double
                 qR[m] = Qx[(m * QROWS + (jR - j0 - QROW0)) * TX + (iR - i0)];
             }
         } else {
-            const long long oL = qoff(a, 0, iL, jL), oR = qoff(a, 0, iR, jR);
 #pragma unroll
             for (int m = 0; m < MEQN; m++) {
                 qL[m] = qin[oL + m * a.plane];
@@ -268,8 +269,8 @@ CLAW2_HD void sweep_chunk(const StepArgs& a, Ctx& ctx, const double* qin, double
         }
 #pragma unroll
         for (int m = 0; m < MAUX; m++) {
-            auxL[m] = a.aux[qoff(a, m, iL, jL)];
-            auxR[m] = a.aux[qoff(a, m, iR, jR)];
+            auxL[m] = a.aux[oL + m * a.plane];
+            auxR[m] = a.aux[oR + m * a.plane];
         }
         RP::template rpn2<IXY>(qL, qR, auxL, auxR, a.prm, wave, s, amdq, apdq, roe);
 #pragma unroll
@@ -283,8 +284,8 @@ CLAW2_HD void sweep_chunk(const StepArgs& a, Ctx& ctx, const double* qin, double
 #pragma unroll
         for (int r = 0; r < NROE; r++) X(2 * MEQN + r, tid) = roe[r];
         if (a.capa >= 0) {
-            dtl = dtn / a.aux[qoff(a, a.capa, iL, jL)];
-            dtr = dtn / a.aux[qoff(a, a.capa, iR, jR)];
+            dtl = dtn / a.aux[oL + a.capa * a.plane];
+            dtr = dtn / a.aux[oR + a.capa * a.plane];
         }
     }
     ctx.syncwarp();
@@ -355,25 +356,26 @@ CLAW2_HD void sweep_chunk(const StepArgs& a, Ctx& ctx, const double* qin, double
                 P[m] = cor ? apdq[m] - cqxx[m] : apdq[m];
             }
             double ax1[AUXN], ax2[AUXN], ax3[AUXN];
-            // ilr = 1: the left-going fluctuation sits in cell k-1
+            // the fluctuation split with ilr = 1 sits in cell k-1, with ilr = 2
+            // in cell k; aux of that cell and of its neighbours across the slice
+            const long long o1 = qoff(a, 0, cell_i(k - 1), cell_j(k - 1));
+            const long long along = IXY == 1 ? 1 : a.ld, across = IXY == 1 ? a.ld : 1;
             {
-                const int ci = cell_i(k - 1), cj = cell_j(k - 1);
 #pragma unroll
                 for (int m = 0; m < MAUX; m++) {
-                    ax1[m] = a.aux[qoff(a, m, IXY == 1 ? ci : ci - 1, IXY == 1 ? cj - 1 : cj)];
-                    ax2[m] = a.aux[qoff(a, m, ci, cj)];
-                    ax3[m] = a.aux[qoff(a, m, IXY == 1 ? ci : ci + 1, IXY == 1 ? cj + 1 : cj)];
+                    ax1[m] = a.aux[o1 - across + m * a.plane];
+                    ax2[m] = a.aux[o1 + m * a.plane];
+                    ax3[m] = a.aux[o1 + across + m * a.plane];
                 }
                 RP::template rpt2<IXY>(1, A, roe, ax1, ax2, ax3, a.prm, bmL, bpL);
             }
-            // ilr = 2: the right-going fluctuation sits in cell k
             {
-                const int ci = cell_i(k), cj = cell_j(k);
+                const long long o2 = o1 + along;
 #pragma unroll
                 for (int m = 0; m < MAUX; m++) {
-                    ax1[m] = a.aux[qoff(a, m, IXY == 1 ? ci : ci - 1, IXY == 1 ? cj - 1 : cj)];
-                    ax2[m] = a.aux[qoff(a, m, ci, cj)];
-                    ax3[m] = a.aux[qoff(a, m, IXY == 1 ? ci : ci + 1, IXY == 1 ? cj + 1 : cj)];
+                    ax1[m] = a.aux[o2 - across + m * a.plane];
+                    ax2[m] = a.aux[o2 + m * a.plane];
+                    ax3[m] = a.aux[o2 + across + m * a.plane];
                 }
                 RP::template rpt2<IXY>(2, P, roe, ax1, ax2, ax3, a.prm, bmR, bpR);
             }
