@@ -139,6 +139,38 @@ def batched_vc_config(n=1024, seed=2024, nmin=64, nmax=384):
     return prob, insts
 
 
+def adjoint_config(n=512, shots=64, nsteps=400, nrec=64, seed=7):
+    """Seismic-style inversion workload on [-1,1]^2, surface at y = 1:
+    variable-coefficient acoustics with a seeded target material (background
+    rho = 1, K = 4 with three circular inclusions of radius 0.3, rho ~ U[1.5,3],
+    K ~ U[2,8]); `shots` sources at random surface cells, each a Ricker pulse
+    (peak frequency 15, delay 0.1) injected into the pressure; `nrec` receivers
+    evenly spaced along the surface; MC, unsplit with transverse_waves=2;
+    extrapolation on the sides and bottom, a wall at the surface; dt fixed by
+    CFL 0.9 of the target material.  Returns a dict of numpy arrays and
+    settings."""
+    rng = np.random.default_rng(seed)
+    x, dx = _centers(-1.0, 1.0, n)
+    y, dy = _centers(-1.0, 1.0, n)
+    X, Y = np.meshgrid(x, y, indexing="ij")
+    rho_t = np.ones((n, n))
+    K_t = np.full((n, n), 4.0)
+    for _ in range(3):
+        cx, cy = rng.uniform(-0.6, 0.6), rng.uniform(-0.7, 0.3)
+        inside = (X - cx) ** 2 + (Y - cy) ** 2 < 0.3 ** 2
+        rho_t[inside] = rng.uniform(1.5, 3.0)
+        K_t[inside] = rng.uniform(2.0, 8.0)
+    c_max = float(np.sqrt(K_t / rho_t).max())
+    dt = 0.9 * min(dx, dy) / c_max
+    t = dt * (np.arange(nsteps) + 1)
+    from pyclaw_b200.adjoint import ricker
+    wav = ricker(t, 15.0, 0.1) / (dx * dy) * dt
+    src = [int(i) + n * (n - 1) for i in rng.integers(0, n, shots)]
+    rec = [int(i) + n * (n - 1) for i in np.linspace(0, n - 1, nrec).round().astype(int)]
+    return dict(n=n, dx=dx, dy=dy, dt=dt, rho_t=rho_t, K_t=K_t, rho0=np.ones((n, n)), K0=np.full((n, n), 4.0),
+                src=src, rec=rec, wav=wav, shots=shots, nsteps=nsteps)
+
+
 def make_solver(pc, prob, run):
     """A ClawSolver2D configured like `prob` (Euler shock-bubble settings)."""
     solver = pc.ClawSolver2D(pc.riemann.rp2_euler_4wave)
@@ -545,6 +577,82 @@ def run_batched(args):
     bs.close()
 
 
+def run_adjoint(args):
+    """The adjoint workload: traces of `shots` shots over `nsteps` steps for the
+    starting material, the L2 misfit against the target material's traces,
+    and its gradient with respect to per-cell (rho, K) and the initial state
+    through the hand-written adjoint (checkpoint every 20 steps).  Times the
+    plain forward, the taped forward and the backward with CUDA events."""
+    import torch
+    from pyclaw_b200.adjoint import AcousticShots, material_aux, shots_traces
+    cfg = adjoint_config(n=args.adj_n, shots=args.adj_shots, nsteps=args.adj_steps)
+    n, S = cfg["n"], cfg["shots"]
+    dev = torch.device("cuda")
+    r = AcousticShots(n, n, cfg["dx"], cfg["dy"], S, cfg["src"], cfg["rec"], cfg["wav"], cfg["dt"],
+                      bc_lower=(1, 1), bc_upper=(1, 3), aux_bc_lower=(1, 1), aux_bc_upper=(1, 1),
+                      order=2, transverse=2, limiters=(4, 4), checkpoint=("uniform", 20))
+    t64 = dict(dtype=torch.float64, device=dev)
+    q0 = torch.zeros((S, 3, n, n), **t64)
+    with torch.no_grad():
+        target = shots_traces(q0, material_aux(torch.tensor(cfg["rho_t"], **t64), torch.tensor(cfg["K_t"], **t64)),
+                              r).clone()
+    rho = torch.tensor(cfg["rho0"], **t64).requires_grad_(True)
+    K = torch.tensor(cfg["K0"], **t64).requires_grad_(True)
+    p0 = torch.zeros((n, n), **t64).requires_grad_(True)
+    z = torch.zeros((n, n), **t64)
+
+    def ev():
+        return torch.cuda.Event(enable_timing=True)
+
+    def once():
+        q = torch.stack([torch.stack([p0, z, z])] * S)
+        e0, e1, e2 = ev(), ev(), ev()
+        e0.record()
+        tr = shots_traces(q, material_aux(rho, K), r)
+        loss = 0.5 * ((tr - target) ** 2).sum()
+        e1.record()
+        loss.backward()
+        e2.record()
+        torch.cuda.synchronize()
+        return loss.item(), e0.elapsed_time(e1) / 1e3, e1.elapsed_time(e2) / 1e3
+
+    def plain_forward():
+        e0, e1 = ev(), ev()
+        st, nx_ = r.new_states(1)[0], r.new_states(1)[0]
+        with torch.no_grad():
+            r.set_aux(material_aux(rho, K))
+            r.set_state(st, torch.stack([torch.stack([p0, z, z])] * S))
+        torch.cuda.synchronize()
+        e0.record()
+        r.advance(st, nx_, 0, cfg["nsteps"])
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / 1e3
+
+    for _ in range(max(1, args.warmup // 3)):
+        once()
+        for x in (rho, K, p0):
+            x.grad = None
+    t_plain = min(plain_forward() for _ in range(2))
+    loss, t_fwd, t_bwd = once()
+    g_rho, g_K, g_p0 = (x.grad for x in (rho, K, p0))
+    cells = n * n * S * cfg["nsteps"]
+    line = {
+        "metric": "adjoint_gradient_cost_over_forward", "value": (t_fwd + t_bwd) / t_plain, "unit": "x",
+        "n_gpus": 1, "steps": cfg["nsteps"], "higher_is_better": False, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "vc_acoustics_adjoint_%dx%d_%dshots_%dsteps" % (n, n, S, cfg["nsteps"]),
+                   "receivers": len(cfg["rec"]), "checkpoint": "uniform every 20 steps",
+                   "inclusions": "3 circles of radius 0.3"},
+        "forward_seconds": t_plain, "taped_forward_seconds": t_fwd, "backward_seconds": t_bwd,
+        "backward_over_forward": t_bwd / t_plain,
+        "forward_cell_updates_per_s": cells / t_plain,
+        "loss": loss,
+        "grad_norms": {"rho": float(g_rho.norm()), "K": float(g_K.norm()), "p0": float(g_p0.norm())},
+        "grad_finite": bool(torch.isfinite(g_rho).all() and torch.isfinite(g_K).all() and torch.isfinite(g_p0).all()),
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -552,14 +660,20 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--workload", default="shockbubble", choices=["shockbubble", "batched"])
+    ap.add_argument("--workload", default="shockbubble", choices=["shockbubble", "batched", "adjoint"])
     ap.add_argument("--instances", type=int, default=1024)
+    ap.add_argument("--adj-n", type=int, default=512)
+    ap.add_argument("--adj-shots", type=int, default=64)
+    ap.add_argument("--adj-steps", type=int, default=400)
     args = ap.parse_args()
     world, rank, local = _dist_init()
     try:
         if args.workload == "batched":
             if rank == 0:
                 run_batched(args)
+        elif args.workload == "adjoint":
+            if rank == 0:
+                run_adjoint(args)
         elif args.impl == "reference":
             run_reference_arm(args, world, rank)
         else:

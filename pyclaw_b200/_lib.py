@@ -2,7 +2,7 @@
 
 There is no fallback: if the library is missing or cannot be loaded, every
 entry point that needs it raises ClawLibraryError.  The prototypes mirror
-include/claw2.h.
+include/claw2.h and include/claw2_adjoint.h.
 """
 import ctypes
 import os
@@ -12,7 +12,7 @@ from . import _abi
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libclaw2.so")
 
-# (name, restype, argtypes) for every function declared in include/claw2.h
+# (name, restype, argtypes) for every function declared in include/*.h
 _P = ctypes.POINTER(_abi.Problem)
 _L = ctypes.POINTER(_abi.Layout)
 _C = ctypes.POINTER(_abi.Control)
@@ -51,6 +51,14 @@ PROTOTYPES = [
     ("claw2_session_step2", ctypes.c_int, [_vp, _dp, _dp, _dp, _dbl, ctypes.POINTER(_dbl)]),
     ("claw2_session_evolve", ctypes.c_int, [_vp, _dp, _dp, ctypes.POINTER(_dbl), ctypes.POINTER(_dbl),
                                             _dbl, _dbl, _dbl, _dbl, _i64, ctypes.POINTER(_dbl)]),
+    # include/claw2_adjoint.h
+    ("claw2_shots_scratch_bytes", ctypes.c_size_t, [_P, ctypes.c_int]),
+    ("claw2_shots_step", ctypes.c_int, [_P, ctypes.c_int, _i64, _dp, _dp, _dp, _dbl, _vp, _dp, _vp]),
+    ("claw2_shots_inject_record", ctypes.c_int, [_P, ctypes.c_int, _i64, _dp, _vp, _dp, ctypes.c_int, _vp, _dp,
+                                                 _vp]),
+    ("claw2_shots_adjoint_step", ctypes.c_int, [_P, ctypes.c_int, _i64, _dp, _dp, _dbl, _dp, _dp, _dp, _i64, _vp]),
+    ("claw2_shots_adjoint_fold", ctypes.c_int, [_P, ctypes.c_int, _i64, _dp, ctypes.c_int, _vp, _dp, _vp]),
+    ("claw2_shots_fold_aux", ctypes.c_int, [_P, ctypes.c_int, _i64, _dp, _vp]),
 ]
 
 

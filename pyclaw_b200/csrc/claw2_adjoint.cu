@@ -1,0 +1,712 @@
+// claw2_adjoint.cu -- multi-shot variable-coefficient acoustics and the
+// hand-written adjoint of its unsplit step (include/claw2_adjoint.h).
+//
+// Forward.  A shot is one wavefield; all shots share aux = (rho, c) and dt.
+// claw2_shots_step runs the fused tile step of claw2_kernels.cuh with the
+// shot as the third grid dimension.
+//
+// Adjoint.  One step of the reference's unsplit method (step2.f90:92-248,
+// flux2.f90:104-206, limiter.f90:34-58, philim.f90:18-55) with the vc-acoustics
+// Riemann solvers, per slice line and interface k (between cells k-1, k):
+//   rpn2:    a1 = (-dp + zR du)/(zL+zR),  a2 = (dp + zL du)/(zL+zR),  z = rho c
+//            W1 = a1 (-zL, 1), s1 = -cL;  W2 = a2 (zR, 1), s2 = cR
+//            amdq = s1 W1, apdq = s2 W2
+//   limiter: L_p = phi(r_p) W_p, r_p = W_p(k).W_p(k -+ 1) / |W_p(k)|^2
+//   cqxx  = sum_p |s_p| (1 - |s_p| dt/dx) L_p,  fadd = cqxx/2
+//   rpt2:    A = amdq + cqxx in cell k-1, P = apdq - cqxx in cell k, each split
+//            into bm = c- b1 (z-, 0, -1)... with the aux of the cell and its two
+//            neighbours across the slice
+//   update:  q(k) += -dtdx (apdq(k) + amdq(k+1)) - dtdx (fadd(k+1) - fadd(k))
+//               - dtdy (g2 - g1) on the own slice, +dtdy g2 / -dtdy g1 on the
+//               slices above / below.
+// The adjoint transposes that map with the limiter branches frozen.  It is
+// organised like the forward: one CTA per AT x AT tile (and shot), one warp
+// per slice line, one lane per interface.  Each CTA recomputes the forward
+// values of every interface its cells depend on and gathers the adjoint into
+// its own cells only, so no two CTAs write the same cell and the result is
+// deterministic.  A cell's state enters only its own row's x-slice and its own
+// column's y-slice, so the lines of a tile are its own rows/columns plus one
+// line on each side whose transverse splits read the tile's aux.
+#include <cuda_runtime.h>
+
+#include <cstring>
+
+#define CLAW2_EXPORT __attribute__((visibility("default")))
+#include "../../include/claw2.h"
+#include "../../include/claw2_adjoint.h"
+#include "claw2_kernels.cuh"
+
+namespace claw2 {
+namespace adj {
+
+constexpr int AT = 27;        // cells per tile side: 32 lanes = interfaces i0-2 .. i0+AT+2
+constexpr int ANT = 256;      // 8 warps
+constexpr int AR = AT + 4;    // shared accumulators: the tile plus a two-cell ghost ring
+constexpr int FT = 29;        // forward tile (the plain step's unsplit tile)
+
+struct AdjArgs {
+    const double* q;          // state at the start of the step, shot 0
+    const double* aux;        // (rho, c)
+    const double* lam_in;     // adjoint of the step's output, shot 0
+    double* lam_out;          // adjoint of the step's input (unfolded), shot 0
+    double* gaux;             // aux gradient accumulator, shot 0
+    long long ld, plane, qstride, gstride;
+    int mx, my;
+    double dtdx, dtdy;
+    int order, trans;
+    int mthlim[2];
+};
+
+__device__ __forceinline__ long long cell(const AdjArgs& a, int i, int j)
+{
+    return (long long)(j + CLAW2_NUM_GHOST) * a.ld + (i + CLAW2_NUM_GHOST);
+}
+
+// philim.f90:18-55 as a function of r, with the derivative of the branch the
+// comparisons select (the same comparisons as philim in claw2_kernels.cuh).
+__device__ __forceinline__ double philim_branch(double r, int meth, double& d)
+{
+    double t, dt, u, du;
+    switch (meth) {
+    case 2:                                            // superbee
+        if (1.0 < 2.0 * r) { t = 1.0; dt = 0.0; } else { t = 2.0 * r; dt = 2.0; }
+        if (2.0 < r) { u = 2.0; du = 0.0; } else { u = r; du = 1.0; }
+        if (!(t > u)) { t = u; dt = du; }
+        if (0.0 > t) { d = 0.0; return 0.0; }
+        d = dt;
+        return t;
+    case 3: {                                          // van Leer
+        const double ar = fabs(r);
+        const double sg = r > 0.0 ? 1.0 : (r < 0.0 ? -1.0 : 0.0);
+        const double den = 1.0 + ar;
+        d = ((1.0 + sg) * den - (r + ar) * sg) / (den * den);
+        return (r + ar) / den;
+    }
+    case 4: {                                          // MC
+        const double c = (1.0 + r) / 2.0;
+        if (c < 2.0) { t = c; dt = 0.5; } else { t = 2.0; dt = 0.0; }
+        if (!(t < 2.0 * r)) { t = 2.0 * r; dt = 2.0; }
+        if (0.0 > t) { d = 0.0; return 0.0; }
+        d = dt;
+        return t;
+    }
+    case 5:
+        d = 1.0;
+        return r;
+    default:                                           // minmod (and ids outside 1..5)
+        if (1.0 < r) { t = 1.0; dt = 0.0; } else { t = r; dt = 1.0; }
+        if (0.0 > t) { d = 0.0; return 0.0; }
+        d = dt;
+        return t;
+    }
+}
+
+// What one lane hands to the cell it owns on its line (cell k, right of its
+// interface): the state adjoint (pressure, normal velocity) and the aux
+// gradient of cell k on the line itself, on the line below and above.
+struct LineOut {
+    double dq_p, dq_n;
+    double ga_own[2], ga_dn[2], ga_up[2];
+};
+
+template <int IXY>
+__device__ __forceinline__ void adj_line(const AdjArgs& a, const double* __restrict__ q,
+                                         const double* __restrict__ lin, int i0, int j0, int line, bool lineok,
+                                         LineOut& o)
+{
+    constexpr int MN = IXY == 1 ? 1 : 2;     // normal velocity component
+    constexpr int MT = IXY == 1 ? 2 : 1;     // transverse velocity component
+    constexpr unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int len = IXY == 1 ? a.mx : a.my;
+    const int k = (IXY == 1 ? i0 : j0) - 2 + lane;
+    const long long P = a.plane;
+    const long long along = IXY == 1 ? 1 : a.ld, across = IXY == 1 ? a.ld : 1;
+    const double dtn = IXY == 1 ? a.dtdx : a.dtdy, dtt = IXY == 1 ? a.dtdy : a.dtdx;
+    const double* __restrict__ aux = a.aux;
+    // the forward solves interfaces -1..len+1 of slices -1..len_other and limits 0..len
+    const bool ex = lineok && k >= -1 && k <= len + 1;
+    const bool lim = ex && a.order == 2 && k >= 0 && k <= len && lane >= 1 && lane <= 30;
+    const long long oR = IXY == 1 ? cell(a, k, line) : cell(a, line, k);
+    const long long oL = oR - along;
+
+    // ---------------- forward recompute: normal solve (RpVcAcoustics::rpn2) ----------------
+    double rhoL = 0.0, cL = 0.0, rhoR = 0.0, cR = 0.0, zL = 0.0, zR = 0.0, d2 = 0.0, den = 1.0, a1 = 0.0, a2 = 0.0;
+    if (ex) {
+        rhoL = aux[oL]; cL = aux[oL + P];
+        rhoR = aux[oR]; cR = aux[oR + P];
+        zR = rhoR * cR;
+        zL = rhoL * cL;
+        const double d1 = q[oR] - q[oL];
+        d2 = q[oR + MN * P] - q[oL + MN * P];
+        den = zL + zR;
+        a1 = (-d1 + zR * d2) / den;
+        a2 = (d1 + zL * d2) / den;
+    }
+    const double w1p = -a1 * zL, w1n = a1, w2p = a2 * zR, w2n = a2;
+    const double s1 = -cL, s2 = cR;
+
+    // neighbours' waves (interfaces k-1 and k+1)
+    const double w1p_l = __shfl_up_sync(FULL, w1p, 1), w1n_l = __shfl_up_sync(FULL, w1n, 1);
+    const double w2p_l = __shfl_up_sync(FULL, w2p, 1), w2n_l = __shfl_up_sync(FULL, w2n, 1);
+    const double w1p_r = __shfl_down_sync(FULL, w1p, 1), w1n_r = __shfl_down_sync(FULL, w1n, 1);
+    const double w2p_r = __shfl_down_sync(FULL, w2p, 1), w2n_r = __shfl_down_sync(FULL, w2n, 1);
+
+    // ---------------- forward recompute: limiter ----------------
+    bool l1 = false, l2 = false;
+    double phi1 = 1.0, phi2 = 1.0, dphi1 = 0.0, dphi2 = 0.0, r1 = 0.0, r2 = 0.0, wn1 = 1.0, wn2 = 1.0;
+    double nb1p = 0.0, nb1n = 0.0, nb2p = 0.0, nb2n = 0.0;
+    if (lim && a.mthlim[0] != 0) {
+        const double wn = w1p * w1p + w1n * w1n;
+        if (wn != 0.0) {
+            l1 = true;
+            wn1 = wn;
+            nb1p = s1 > 0.0 ? w1p_l : w1p_r;
+            nb1n = s1 > 0.0 ? w1n_l : w1n_r;
+            r1 = (w1p * nb1p + w1n * nb1n) / wn;
+            phi1 = philim_branch(r1, a.mthlim[0], dphi1);
+        }
+    }
+    if (lim && a.mthlim[1] != 0) {
+        const double wn = w2p * w2p + w2n * w2n;
+        if (wn != 0.0) {
+            l2 = true;
+            wn2 = wn;
+            nb2p = s2 > 0.0 ? w2p_l : w2p_r;
+            nb2n = s2 > 0.0 ? w2n_l : w2n_r;
+            r2 = (w2p * nb2p + w2n * nb2n) / wn;
+            phi2 = philim_branch(r2, a.mthlim[1], dphi2);
+        }
+    }
+    const bool second = a.order == 2;
+    const double dtave = 0.5 * (dtn + dtn);
+    const double as1 = fabs(s1), as2 = fabs(s2);
+    const double f1 = as1 * (1.0 - as1 * dtave), f2 = as2 * (1.0 - as2 * dtave);
+    const double L1p = phi1 * w1p, L1n = phi1 * w1n, L2p = phi2 * w2p, L2n = phi2 * w2n;
+    const double cqp = second ? f1 * L1p + f2 * L2p : 0.0;
+    const bool cor = second && a.trans == 2;
+    const double Ap = s1 * w1p + (cor ? cqp : 0.0);     // asdq(1) of the two transverse splits
+    const double Pp = s2 * w2p - (cor ? cqp : 0.0);
+
+    // ---------------- adjoint of the update: the interface's outputs ----------------
+    // lambda at cells k-1 (A) and k (B) on the line and the lines below/above
+    double LAp0 = 0, LAt0 = 0, LAp1 = 0, LAn1 = 0, LAt1 = 0, LAp2 = 0, LAt2 = 0;
+    double LBp0 = 0, LBt0 = 0, LBp1 = 0, LBn1 = 0, LBt1 = 0, LBp2 = 0, LBt2 = 0;
+    if (ex) {
+        LAp1 = lin[oL]; LAn1 = lin[oL + MN * P]; LAt1 = lin[oL + MT * P];
+        LBp1 = lin[oR]; LBn1 = lin[oR + MN * P]; LBt1 = lin[oR + MT * P];
+        if (a.trans > 0) {
+            LAp0 = lin[oL - across]; LAt0 = lin[oL - across + MT * P];
+            LAp2 = lin[oL + across]; LAt2 = lin[oL + across + MT * P];
+            LBp0 = lin[oR - across]; LBt0 = lin[oR - across + MT * P];
+            LBp2 = lin[oR + across]; LBt2 = lin[oR + across + MT * P];
+        }
+    }
+    double gAm_p = -dtn * LAp1, gAm_n = -dtn * LAn1;            // d/d amdq
+    double gAp_p = -dtn * LBp1, gAp_n = -dtn * LBn1;            // d/d apdq
+    const double gF_p = -dtn * (LAp1 - LBp1), gF_n = -dtn * (LAn1 - LBn1);   // d/d fadd
+
+    // ---------------- transverse splits (RpVcAcoustics::rpt2), transposed ----------------
+    // aux gradient of cell k-1 (A) and cell k (B) on lines -1, 0, +1
+    double gA_r0 = 0, gA_c0 = 0, gA_r1 = 0, gA_c1 = 0, gA_r2 = 0, gA_c2 = 0;
+    double gB_r0 = 0, gB_c0 = 0, gB_r1 = 0, gB_c1 = 0, gB_r2 = 0, gB_c2 = 0;
+    double gApd = 0.0, gPpd = 0.0;                               // d/d asdq(1)
+    if (ex && a.trans > 0) {
+        const double h = 0.5 * dtn;
+        // g1(c) = dtt (lam(c) - lam(c, below)), g2(c) = dtt (lam(c, above) - lam(c))
+        auto split_T = [&](double asdq, double lp0, double lt0, double lp1, double lt1, double lp2, double lt2,
+                           long long oc, double& g_r0, double& g_c0, double& g_r1, double& g_c1, double& g_r2,
+                           double& g_c2) -> double {
+            const double bm_p = -h * (dtt * (lp1 - lp0)), bm_t = -h * (dtt * (lt1 - lt0));   // d/d bmasdq
+            const double bp_p = -h * (dtt * (lp2 - lp1)), bp_t = -h * (dtt * (lt2 - lt1));   // d/d bpasdq
+            const double rho0 = aux[oc - across], c0 = aux[oc - across + P];
+            const double rho1 = aux[oc], c1 = aux[oc + P];
+            const double rho2 = aux[oc + across], c2 = aux[oc + across + P];
+            const double zm = rho0 * c0, zz = rho1 * c1, zp = rho2 * c2;
+            const double D1 = zm + zz, D2 = zz + zp;
+            const double b1 = -asdq / D1, b2 = asdq / D2;
+            const double db1 = c0 * zm * bm_p - c0 * bm_t;
+            const double db2 = c2 * zp * bp_p + c2 * bp_t;
+            const double dcm = b1 * zm * bm_p - b1 * bm_t;
+            const double dcp = b2 * zp * bp_p + b2 * bp_t;
+            const double dD1 = -b1 * db1 / D1, dD2 = -b2 * db2 / D2;
+            const double dzm = c0 * b1 * bm_p + dD1;
+            const double dzp = c2 * b2 * bp_p + dD2;
+            const double dzz = dD1 + dD2;
+            g_r0 = c0 * dzm; g_c0 = rho0 * dzm + dcm;
+            g_r1 = c1 * dzz; g_c1 = rho1 * dzz;
+            g_r2 = c2 * dzp; g_c2 = rho2 * dzp + dcp;
+            return -db1 / D1 + db2 / D2;
+        };
+        gApd = split_T(Ap, LAp0, LAt0, LAp1, LAt1, LAp2, LAt2, oL, gA_r0, gA_c0, gA_r1, gA_c1, gA_r2, gA_c2);
+        gPpd = split_T(Pp, LBp0, LBt0, LBp1, LBt1, LBp2, LBt2, oR, gB_r0, gB_c0, gB_r1, gB_c1, gB_r2, gB_c2);
+    }
+    gAm_p += gApd;
+    gAp_p += gPpd;
+
+    // ---------------- correction fluxes and limiter, transposed ----------------
+    double gW1p = s1 * gAm_p, gW1n = s1 * gAm_n, gW2p = s2 * gAp_p, gW2n = s2 * gAp_n;
+    double gs1 = w1p * gAm_p + w1n * gAm_n, gs2 = w2p * gAp_p + w2n * gAp_n;
+    double send1p = 0.0, send1n = 0.0, send2p = 0.0, send2n = 0.0;   // to the upwind neighbour's wave
+    if (ex && second) {
+        const double gcq_p = 0.5 * gF_p + (cor ? gApd - gPpd : 0.0);
+        const double gcq_n = 0.5 * gF_n;
+        const double gL1p = f1 * gcq_p, gL1n = f1 * gcq_n, gL2p = f2 * gcq_p, gL2n = f2 * gcq_n;
+        const double gf1 = L1p * gcq_p + L1n * gcq_n, gf2 = L2p * gcq_p + L2n * gcq_n;
+        const double sg1 = s1 > 0.0 ? 1.0 : (s1 < 0.0 ? -1.0 : 0.0);
+        const double sg2 = s2 > 0.0 ? 1.0 : (s2 < 0.0 ? -1.0 : 0.0);
+        gs1 += sg1 * (1.0 - 2.0 * as1 * dtave) * gf1;
+        gs2 += sg2 * (1.0 - 2.0 * as2 * dtave) * gf2;
+        gW1p += phi1 * gL1p; gW1n += phi1 * gL1n;
+        gW2p += phi2 * gL2p; gW2n += phi2 * gL2n;
+        if (l1) {
+            const double gr = dphi1 * (w1p * gL1p + w1n * gL1n);
+            const double gdot = gr / wn1, gwn = -r1 * gr / wn1;
+            gW1p += 2.0 * gwn * w1p + gdot * nb1p;
+            gW1n += 2.0 * gwn * w1n + gdot * nb1n;
+            send1p = gdot * w1p; send1n = gdot * w1n;
+        }
+        if (l2) {
+            const double gr = dphi2 * (w2p * gL2p + w2n * gL2n);
+            const double gdot = gr / wn2, gwn = -r2 * gr / wn2;
+            gW2p += 2.0 * gwn * w2p + gdot * nb2p;
+            gW2n += 2.0 * gwn * w2n + gdot * nb2n;
+            send2p = gdot * w2p; send2n = gdot * w2n;
+        }
+    }
+    {
+        // a wave with s > 0 read its left neighbour, otherwise its right one
+        const bool left1 = s1 > 0.0, left2 = s2 > 0.0;
+        const double tl1p = left1 ? send1p : 0.0, tl1n = left1 ? send1n : 0.0;
+        const double tr1p = left1 ? 0.0 : send1p, tr1n = left1 ? 0.0 : send1n;
+        const double tl2p = left2 ? send2p : 0.0, tl2n = left2 ? send2n : 0.0;
+        const double tr2p = left2 ? 0.0 : send2p, tr2n = left2 ? 0.0 : send2n;
+        const double fr1p = __shfl_down_sync(FULL, tl1p, 1), fr1n = __shfl_down_sync(FULL, tl1n, 1);
+        const double fr2p = __shfl_down_sync(FULL, tl2p, 1), fr2n = __shfl_down_sync(FULL, tl2n, 1);
+        const double fl1p = __shfl_up_sync(FULL, tr1p, 1), fl1n = __shfl_up_sync(FULL, tr1n, 1);
+        const double fl2p = __shfl_up_sync(FULL, tr2p, 1), fl2n = __shfl_up_sync(FULL, tr2n, 1);
+        if (lane < 31) { gW1p += fr1p; gW1n += fr1n; gW2p += fr2p; gW2n += fr2n; }
+        if (lane > 0) { gW1p += fl1p; gW1n += fl1n; gW2p += fl2p; gW2n += fl2n; }
+    }
+
+    // ---------------- normal solve, transposed ----------------
+    double gqR_p = 0, gqR_n = 0, gqL_p = 0, gqL_n = 0, grL = 0, gcL = 0, grR = 0, gcR = 0;
+    if (ex) {
+        const double ga1 = -zL * gW1p + gW1n;
+        const double ga2 = zR * gW2p + gW2n;
+        double gzL = -a1 * gW1p, gzR = a2 * gW2p;
+        const double inv = 1.0 / den;
+        const double gd1 = (ga2 - ga1) * inv;
+        const double gd2 = (zR * ga1 + zL * ga2) * inv;
+        gzR += d2 * ga1 * inv;
+        gzL += d2 * ga2 * inv;
+        const double gden = -(a1 * ga1 + a2 * ga2) * inv;
+        gzL += gden;
+        gzR += gden;
+        gqR_p = gd1; gqL_p = -gd1;
+        gqR_n = gd2; gqL_n = -gd2;
+        grL = cL * gzL; gcL = -gs1 + rhoL * gzL;
+        grR = cR * gzR; gcR = gs2 + rhoR * gzR;
+    }
+
+    // ---------------- gather onto cell k (this lane) from interfaces k and k+1 ----------------
+    const double nq_p = __shfl_down_sync(FULL, gqL_p, 1), nq_n = __shfl_down_sync(FULL, gqL_n, 1);
+    const double nown_r = __shfl_down_sync(FULL, grL + gA_r1, 1), nown_c = __shfl_down_sync(FULL, gcL + gA_c1, 1);
+    const double ndn_r = __shfl_down_sync(FULL, gA_r0, 1), ndn_c = __shfl_down_sync(FULL, gA_c0, 1);
+    const double nup_r = __shfl_down_sync(FULL, gA_r2, 1), nup_c = __shfl_down_sync(FULL, gA_c2, 1);
+    o.dq_p = gqR_p + nq_p;
+    o.dq_n = gqR_n + nq_n;
+    o.ga_own[0] = (grR + gB_r1) + nown_r;
+    o.ga_own[1] = (gcR + gB_c1) + nown_c;
+    o.ga_dn[0] = gB_r0 + ndn_r;
+    o.ga_dn[1] = gB_c0 + ndn_c;
+    o.ga_up[0] = gB_r2 + nup_r;
+    o.ga_up[1] = gB_c2 + nup_c;
+}
+
+__global__ void __launch_bounds__(ANT, 1) adjoint_kernel(AdjArgs a)
+{
+    __shared__ double GQ[3 * AR * AR];
+    __shared__ double GA[2 * AR * AR];
+    const int shot = blockIdx.z;
+    const double* __restrict__ q = a.q + shot * a.qstride;
+    const double* __restrict__ lin = a.lam_in + shot * a.qstride;
+    double* lout = a.lam_out + shot * a.qstride;
+    double* gaux = a.gaux + shot * a.gstride;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int i0 = blockIdx.x * AT, j0 = blockIdx.y * AT;
+    // cells this CTA owns: its tile, plus the ghost ring on domain sides
+    const int ilo = i0 == 0 ? -2 : i0, ihi = i0 + AT >= a.mx ? a.mx + 2 : i0 + AT;
+    const int jlo = j0 == 0 ? -2 : j0, jhi = j0 + AT >= a.my ? a.my + 2 : j0 + AT;
+    const long long P = a.plane;
+    auto sidx = [&](int i, int j) { return (j - j0 + 2) * AR + (i - i0 + 2); };
+
+    for (int t = tid; t < AR * AR; t += ANT) {
+        const int i = i0 - 2 + t % AR, j = j0 - 2 + t / AR;
+        const bool interior = i >= 0 && i < a.mx && j >= 0 && j < a.my && i < ihi && j < jhi;
+        const long long o = cell(a, i, j);
+#pragma unroll
+        for (int m = 0; m < 3; m++) GQ[m * AR * AR + t] = interior ? lin[o + m * P] : 0.0;   // identity term
+        GA[t] = 0.0;
+        GA[AR * AR + t] = 0.0;
+    }
+    __syncthreads();
+
+    // ---- x-slices: rows j0-1 .. j0+AT (the forward has rows -1 .. my)
+    {
+        const int first = j0 - 1 > -1 ? j0 - 1 : -1;
+        const int last = j0 + AT < a.my ? j0 + AT : a.my;
+        for (int c0 = first; c0 <= last; c0 += ANT / 32) {
+            const int line = c0 + warp;
+            const bool ok = line <= last;
+            LineOut o;
+            adj_line<1>(a, q, lin, i0, j0, line, ok, o);
+            const int c = i0 - 2 + lane;
+            const bool cown = ok && c >= ilo && c < ihi;
+            if (cown && line >= jlo && line < jhi) {
+                const int s = sidx(c, line);
+                GQ[s] += o.dq_p;
+                GQ[AR * AR + s] += o.dq_n;
+                GA[s] += o.ga_own[0];
+                GA[AR * AR + s] += o.ga_own[1];
+            }
+            __syncthreads();
+            if (cown && line + 1 >= jlo && line + 1 < jhi) {
+                const int s = sidx(c, line + 1);
+                GA[s] += o.ga_up[0];
+                GA[AR * AR + s] += o.ga_up[1];
+            }
+            __syncthreads();
+            if (cown && line - 1 >= jlo && line - 1 < jhi) {
+                const int s = sidx(c, line - 1);
+                GA[s] += o.ga_dn[0];
+                GA[AR * AR + s] += o.ga_dn[1];
+            }
+            __syncthreads();
+        }
+    }
+    // ---- y-slices: columns i0-1 .. i0+AT
+    {
+        const int first = i0 - 1 > -1 ? i0 - 1 : -1;
+        const int last = i0 + AT < a.mx ? i0 + AT : a.mx;
+        for (int c0 = first; c0 <= last; c0 += ANT / 32) {
+            const int line = c0 + warp;
+            const bool ok = line <= last;
+            LineOut o;
+            adj_line<2>(a, q, lin, i0, j0, line, ok, o);
+            const int c = j0 - 2 + lane;
+            const bool cown = ok && c >= jlo && c < jhi;
+            if (cown && line >= ilo && line < ihi) {
+                const int s = sidx(line, c);
+                GQ[s] += o.dq_p;
+                GQ[2 * AR * AR + s] += o.dq_n;
+                GA[s] += o.ga_own[0];
+                GA[AR * AR + s] += o.ga_own[1];
+            }
+            __syncthreads();
+            if (cown && line + 1 >= ilo && line + 1 < ihi) {
+                const int s = sidx(line + 1, c);
+                GA[s] += o.ga_up[0];
+                GA[AR * AR + s] += o.ga_up[1];
+            }
+            __syncthreads();
+            if (cown && line - 1 >= ilo && line - 1 < ihi) {
+                const int s = sidx(line - 1, c);
+                GA[s] += o.ga_dn[0];
+                GA[AR * AR + s] += o.ga_dn[1];
+            }
+            __syncthreads();
+        }
+    }
+
+    for (int t = tid; t < AR * AR; t += ANT) {
+        const int i = i0 - 2 + t % AR, j = j0 - 2 + t / AR;
+        if (i < ilo || i >= ihi || j < jlo || j >= jhi) continue;
+        const long long o = cell(a, i, j);
+#pragma unroll
+        for (int m = 0; m < 3; m++) lout[o + m * P] = GQ[m * AR * AR + t];
+        gaux[o] += GA[t];
+        gaux[o + P] += GA[AR * AR + t];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// forward: the plain tile step with the shot as third grid dimension
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256, 2) shots_step_kernel(StepArgs common, long long qstride)
+{
+    extern __shared__ double smem_dyn[];
+    DevCtx ctx{smem_dyn};
+    const int shot = blockIdx.z;
+    StepArgs a = common;
+    a.qin += shot * qstride;
+    a.qout += shot * qstride;
+    a.partials += (long long)shot * gridDim.x * gridDim.y;
+    a.ticket += shot;
+    a.cfl_out += shot;
+    const TileId t{(int)blockIdx.x, (int)blockIdx.y, (int)gridDim.x, (int)gridDim.y,
+                   (int)(blockIdx.y * gridDim.x + blockIdx.x), (int)(gridDim.x * gridDim.y)};
+    step_tile_at<RpVcAcoustics, FT, FT, 256, false>(a, ctx, t);
+}
+
+struct ShotIO {
+    double* q;
+    long long ld, plane, qstride;
+    int mx, my, nrec;
+    int bcl[2], bcu[2];
+    const int32_t* src;
+    const double* amp;
+    const int32_t* rec;
+    double* traces;
+};
+
+// one CTA per shot: the source, its ghost images, then the receivers
+__global__ void inject_record_kernel(ShotIO s)
+{
+    const int shot = blockIdx.x;
+    double* p = s.q + shot * s.qstride;          // pressure plane of this shot
+    auto off = [&](int i, int j) { return (long long)(j + CLAW2_NUM_GHOST) * s.ld + (i + CLAW2_NUM_GHOST); };
+    const int ncell = s.mx * s.my;
+    if (threadIdx.x == 0 && s.amp && s.src[shot] >= 0 && s.src[shot] < ncell) {
+        const int i = s.src[shot] % s.mx, j = s.src[shot] / s.mx;
+        const double v = p[off(i, j)] + s.amp[shot];
+        p[off(i, j)] = v;
+        int gx[2], gy[2];
+        bool nx[2], ny[2];
+        const int kx = ghost_images(i, s.mx, s.bcl[0], s.bcu[0], gx, nx);
+        const int ky = ghost_images(j, s.my, s.bcl[1], s.bcu[1], gy, ny);
+        for (int u = 0; u < kx; u++) p[off(gx[u], j)] = v;
+        for (int w = 0; w < ky; w++) p[off(i, gy[w])] = v;
+        for (int u = 0; u < kx; u++)
+            for (int w = 0; w < ky; w++) p[off(gx[u], gy[w])] = v;
+    }
+    __syncthreads();
+    if (s.traces)
+        for (int r = threadIdx.x; r < s.nrec; r += blockDim.x) {
+            const int c = s.rec[r];
+            s.traces[(long long)shot * s.nrec + r] = (c >= 0 && c < ncell) ? p[off(c % s.mx, c / s.mx)] : 0.0;
+        }
+}
+
+struct FoldArgs {
+    double* x;
+    long long ld, plane, stride;
+    int mx, my, ncomp;
+    int bcl[2], bcu[2];
+    int negate;                 // 1: walls negate the normal velocity (state); 0: aux
+    int nrec;
+    const int32_t* rec;
+    const double* gtrace;
+};
+
+// Transpose of one side's ghost fill along one axis (fill_body in claw2_capi.cu):
+// the adjoint of each ghost cell goes back to its source cell, then is zeroed.
+template <int AXIS>
+__device__ __forceinline__ void fold_axis(const FoldArgs& f, double* x)
+{
+    const int n = AXIS == 0 ? f.mx : f.my;
+    // along the other axis: y-fold covers all columns (ghosts too), x-fold the interior rows
+    const int olo = AXIS == 1 ? -CLAW2_NUM_GHOST : 0;
+    const int ohi = AXIS == 1 ? f.mx + CLAW2_NUM_GHOST : f.my;
+    const int nother = ohi - olo;
+    const int total = f.ncomp * nother * 2;
+    for (int t = threadIdx.x; t < total; t += blockDim.x) {
+        const int o = olo + t % nother;
+        const int side = (t / nother) % 2;
+        const int m = t / (2 * nother);
+        const int bc = side == 0 ? f.bcl[AXIS] : f.bcu[AXIS];
+        auto off = [&](int along) {
+            const int i = AXIS == 0 ? along : o, j = AXIS == 0 ? o : along;
+            return (long long)m * f.plane + (long long)(j + CLAW2_NUM_GHOST) * f.ld + (i + CLAW2_NUM_GHOST);
+        };
+        for (int g = 0; g < CLAW2_NUM_GHOST; g++) {
+            int dst, src;
+            if (side == 0) {
+                dst = -1 - g;
+                src = bc == CLAW2_BC_EXTRAP ? 0 : (bc == CLAW2_BC_PERIODIC ? n - 1 - g : g);
+            } else {
+                dst = n + g;
+                src = bc == CLAW2_BC_EXTRAP ? n - 1 : (bc == CLAW2_BC_PERIODIC ? g : n - 1 - g);
+            }
+            double v = x[off(dst)];
+            if (bc == CLAW2_BC_WALL && f.negate && m == AXIS + 1) v = -v;
+            x[off(src)] += v;
+            x[off(dst)] = 0.0;
+        }
+    }
+}
+
+// one CTA per shot
+__global__ void fold_kernel(FoldArgs f)
+{
+    double* x = f.x + blockIdx.x * f.stride;
+    fold_axis<1>(f, x);         // the y fill ran last, so its transpose runs first
+    __syncthreads();
+    fold_axis<0>(f, x);
+    __syncthreads();
+    if (f.gtrace && threadIdx.x == 0)
+        for (int r = 0; r < f.nrec; r++) {
+            const int c = f.rec[r];
+            if (c < 0 || c >= f.mx * f.my) continue;
+            x[(long long)(c / f.mx + CLAW2_NUM_GHOST) * f.ld + (c % f.mx + CLAW2_NUM_GHOST)] +=
+                f.gtrace[(long long)blockIdx.x * f.nrec + r];
+        }
+}
+
+}  // namespace adj
+}  // namespace claw2
+
+using namespace claw2;
+using namespace claw2::adj;
+
+namespace {
+
+int shots_check(const claw2_problem* p, int nshots)
+{
+    if (!p || nshots < 1) return CLAW2_ERR_INVALID;
+    int rc = claw2_validate(p);
+    if (rc) return rc;
+    if (p->rp != CLAW2_RP_VC_ACOUSTICS || p->transverse < 0 || p->index_capa >= 0 || p->use_fwave)
+        return CLAW2_ERR_UNSUPPORTED;
+    if (p->mx < 4 || p->my < 4) return CLAW2_ERR_UNSUPPORTED;
+    for (int d = 0; d < 2; d++) {
+        if (p->bc_lower[d] == CLAW2_BC_CUSTOM || p->bc_upper[d] == CLAW2_BC_CUSTOM) return CLAW2_ERR_UNSUPPORTED;
+        if (p->aux_bc_lower[d] == CLAW2_BC_CUSTOM || p->aux_bc_upper[d] == CLAW2_BC_CUSTOM) return CLAW2_ERR_UNSUPPORTED;
+        if ((p->aux_bc_lower[d] == CLAW2_BC_PERIODIC) != (p->aux_bc_upper[d] == CLAW2_BC_PERIODIC))
+            return CLAW2_ERR_UNSUPPORTED;
+    }
+    return CLAW2_OK;
+}
+
+int ftiles(const claw2_problem* p, int* nbx, int* nby)
+{
+    *nbx = (p->mx + FT - 1) / FT;
+    *nby = (p->my + FT - 1) / FT;
+    return *nbx * *nby;
+}
+
+inline cudaStream_t Sx(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+}  // namespace
+
+extern "C" {
+
+size_t claw2_shots_scratch_bytes(const claw2_problem* p, int nshots)
+{
+    if (!p || nshots < 1 || p->mx < 1 || p->my < 1) return 0;
+    int nbx, nby;
+    const size_t nt = (size_t)ftiles(p, &nbx, &nby);
+    const size_t tickets = ((size_t)nshots * sizeof(unsigned int) + 255) / 256 * 256;
+    return tickets + sizeof(double) * nt * (size_t)nshots;
+}
+
+int claw2_shots_step(const claw2_problem* p, int nshots, long long shot_stride, const double* q_in, double* q_out,
+                     const double* aux, double dt, void* scratch, double* cfl_dev, void* stream)
+{
+    int rc = shots_check(p, nshots);
+    if (rc) return rc;
+    if (!q_in || !q_out || !aux || !scratch || !cfl_dev || q_in == q_out) return CLAW2_ERR_INVALID;
+    claw2_layout L;
+    claw2_get_layout(p, &L);
+    if (shot_stride < L.q_elems && nshots > 1) return CLAW2_ERR_INVALID;
+    StepArgs a;
+    std::memset(&a, 0, sizeof a);
+    a.qin = q_in; a.qout = q_out; a.aux = aux; a.dt = dt;
+    a.ld = L.ld; a.plane = L.plane; a.mx = p->mx; a.my = p->my; a.dx = p->dx; a.dy = p->dy;
+    a.order = p->order; a.trans = p->transverse; a.capa = -1; a.fwave = 0;
+    for (int w = 0; w < 2; w++) {
+        a.mthlim[w] = p->mthlim[w];
+        if (p->mthlim[w] > 0) a.limit_any = 1;
+    }
+    a.ghost_fused = 1;
+    for (int d = 0; d < 2; d++) { a.bcl[d] = p->bc_lower[d]; a.bcu[d] = p->bc_upper[d]; }
+    const size_t tickets = ((size_t)nshots * sizeof(unsigned int) + 255) / 256 * 256;
+    a.ticket = static_cast<unsigned int*>(scratch);
+    a.partials = reinterpret_cast<double*>(static_cast<char*>(scratch) + tickets);
+    a.cfl_out = cfl_dev;
+    using SM = TileSmem<RpVcAcoustics, FT, FT, 256, false>;
+    static bool configured = false;
+    if (!configured) {
+        if (cudaFuncSetAttribute(shots_step_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SM::bytes) !=
+            cudaSuccess)
+            return CLAW2_ERR_CUDA;
+        configured = true;
+    }
+    int nbx, nby;
+    ftiles(p, &nbx, &nby);
+    shots_step_kernel<<<dim3(nbx, nby, nshots), 256, SM::bytes, Sx(stream)>>>(a, shot_stride);
+    return cudaGetLastError() == cudaSuccess ? CLAW2_OK : CLAW2_ERR_CUDA;
+}
+
+int claw2_shots_inject_record(const claw2_problem* p, int nshots, long long shot_stride, double* q,
+                              const int32_t* src_cell, const double* src_amp, int nrec, const int32_t* rec_cell,
+                              double* traces, void* stream)
+{
+    int rc = shots_check(p, nshots);
+    if (rc) return rc;
+    if (!q || nrec < 0 || (src_amp && !src_cell) || (traces && nrec > 0 && !rec_cell)) return CLAW2_ERR_INVALID;
+    claw2_layout L;
+    claw2_get_layout(p, &L);
+    ShotIO s;
+    s.q = q; s.ld = L.ld; s.plane = L.plane; s.qstride = shot_stride; s.mx = p->mx; s.my = p->my; s.nrec = nrec;
+    for (int d = 0; d < 2; d++) { s.bcl[d] = p->bc_lower[d]; s.bcu[d] = p->bc_upper[d]; }
+    s.src = src_cell; s.amp = src_amp; s.rec = rec_cell; s.traces = nrec > 0 ? traces : nullptr;
+    inject_record_kernel<<<nshots, 128, 0, Sx(stream)>>>(s);
+    return cudaGetLastError() == cudaSuccess ? CLAW2_OK : CLAW2_ERR_CUDA;
+}
+
+int claw2_shots_adjoint_step(const claw2_problem* p, int nshots, long long shot_stride, const double* q,
+                             const double* aux, double dt, const double* lam_in, double* lam_out, double* gaux,
+                             long long gaux_stride, void* stream)
+{
+    int rc = shots_check(p, nshots);
+    if (rc) return rc;
+    if (!q || !aux || !lam_in || !lam_out || !gaux || lam_in == lam_out) return CLAW2_ERR_INVALID;
+    claw2_layout L;
+    claw2_get_layout(p, &L);
+    if (nshots > 1 && (shot_stride < L.q_elems || gaux_stride < 2 * L.plane)) return CLAW2_ERR_INVALID;
+    AdjArgs a;
+    a.q = q; a.aux = aux; a.lam_in = lam_in; a.lam_out = lam_out; a.gaux = gaux;
+    a.ld = L.ld; a.plane = L.plane; a.qstride = shot_stride; a.gstride = gaux_stride;
+    a.mx = p->mx; a.my = p->my;
+    a.dtdx = dt / p->dx; a.dtdy = dt / p->dy;
+    a.order = p->order; a.trans = p->transverse;
+    a.mthlim[0] = p->mthlim[0]; a.mthlim[1] = p->mthlim[1];
+    const dim3 grid((p->mx + AT - 1) / AT, (p->my + AT - 1) / AT, nshots);
+    adjoint_kernel<<<grid, ANT, 0, Sx(stream)>>>(a);
+    return cudaGetLastError() == cudaSuccess ? CLAW2_OK : CLAW2_ERR_CUDA;
+}
+
+static int fold_launch(const claw2_problem* p, int nshots, long long stride, double* x, int ncomp, const int* bl,
+                       const int* bu, int negate, int nrec, const int32_t* rec, const double* gtrace, void* stream)
+{
+    claw2_layout L;
+    claw2_get_layout(p, &L);
+    FoldArgs f;
+    f.x = x; f.ld = L.ld; f.plane = L.plane; f.stride = stride; f.mx = p->mx; f.my = p->my; f.ncomp = ncomp;
+    for (int d = 0; d < 2; d++) { f.bcl[d] = bl[d]; f.bcu[d] = bu[d]; }
+    f.negate = negate; f.nrec = nrec; f.rec = rec; f.gtrace = gtrace;
+    fold_kernel<<<nshots, 256, 0, Sx(stream)>>>(f);
+    return cudaGetLastError() == cudaSuccess ? CLAW2_OK : CLAW2_ERR_CUDA;
+}
+
+int claw2_shots_adjoint_fold(const claw2_problem* p, int nshots, long long shot_stride, double* lam, int nrec,
+                             const int32_t* rec_cell, const double* gtrace, void* stream)
+{
+    int rc = shots_check(p, nshots);
+    if (rc) return rc;
+    if (!lam || nrec < 0 || (gtrace && nrec > 0 && !rec_cell)) return CLAW2_ERR_INVALID;
+    return fold_launch(p, nshots, shot_stride, lam, 3, p->bc_lower, p->bc_upper, 1, nrec, rec_cell,
+                       nrec > 0 ? gtrace : nullptr, stream);
+}
+
+int claw2_shots_fold_aux(const claw2_problem* p, int nshots, long long gaux_stride, double* gaux, void* stream)
+{
+    int rc = shots_check(p, nshots);
+    if (rc) return rc;
+    if (!gaux) return CLAW2_ERR_INVALID;
+    return fold_launch(p, nshots, gaux_stride, gaux, 2, p->aux_bc_lower, p->aux_bc_upper, 0, 0, nullptr, nullptr,
+                       stream);
+}
+
+}  // extern "C"

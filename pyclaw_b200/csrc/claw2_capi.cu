@@ -17,25 +17,6 @@
 
 namespace claw2 {
 
-// ---------------------------------------------------------------------------
-// device execution context for step_tile
-// ---------------------------------------------------------------------------
-struct DevCtx {
-    double* sm;
-    __device__ __forceinline__ int tid() const { return threadIdx.x; }
-    __device__ __forceinline__ int bx() const { return blockIdx.x; }
-    __device__ __forceinline__ int by() const { return blockIdx.y; }
-    __device__ __forceinline__ int nbx() const { return gridDim.x; }
-    __device__ __forceinline__ int nby() const { return gridDim.y; }
-    __device__ __forceinline__ void sync() const { __syncthreads(); }
-    __device__ __forceinline__ void syncwarp() const { __syncwarp(); }
-    __device__ __forceinline__ void fence() const { __threadfence(); }
-    __device__ __forceinline__ unsigned atomic_inc(unsigned* p) const { return atomicAdd(p, 1u); }
-    __device__ __forceinline__ double load_volatile(const double* p) const { return *(volatile const double*)p; }
-    __device__ __forceinline__ double nan() const { return __longlong_as_double(0x7ff8000000000000ULL); }
-    __device__ __forceinline__ double* smem() const { return sm; }
-};
-
 #ifndef CLAW2_MINB
 #define CLAW2_MINB 2        // resident CTAs per SM the register budget is sized for
 #endif

@@ -1,5 +1,5 @@
 """Host-side checks of the C ABI (no GPU needed): the library loads, exports
-every function include/claw2.h declares, and its host-only entry points
+every function include/*.h declares, and its host-only entry points
 (validation, layout, scratch size, controller initialisation) behave."""
 import ctypes
 import os
@@ -15,9 +15,13 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
 def declared_functions():
-    with open(os.path.join(ROOT, "include", "claw2.h")) as f:
-        src = f.read()
-    return sorted(set(re.findall(r"CLAW2_EXPORT\s+(?:const\s+)?\w+\*?\s+(claw2_\w+)\s*\(", src)))
+    names = set()
+    inc = os.path.join(ROOT, "include")
+    for h in sorted(os.listdir(inc)):
+        if h.endswith(".h"):
+            with open(os.path.join(inc, h)) as f:
+                names.update(re.findall(r"CLAW2_EXPORT\s+(?:const\s+)?\w+\*?\s+(claw2_\w+)\s*\(", f.read()))
+    return sorted(names)
 
 
 def test_header_declares_the_prototypes_python_binds():
