@@ -43,6 +43,9 @@ constexpr int AT = 27;        // cells per tile side: 32 lanes = interfaces i0-2
 constexpr int ANT = 256;      // 8 warps
 constexpr int AR = AT + 4;    // shared accumulators: the tile plus a two-cell ghost ring
 constexpr int FT = 29;        // forward tile (the plain step's unsplit tile)
+#ifndef CLAW2_ADJ_MINB
+#define CLAW2_ADJ_MINB 2      // resident CTAs per SM the register budget is sized for
+#endif
 
 struct AdjArgs {
     const double* q;          // state at the start of the step, shot 0
@@ -223,20 +226,20 @@ __device__ __forceinline__ void adj_line(const AdjArgs& a, const double* __restr
             const double rho1 = aux[oc], c1 = aux[oc + P];
             const double rho2 = aux[oc + across], c2 = aux[oc + across + P];
             const double zm = rho0 * c0, zz = rho1 * c1, zp = rho2 * c2;
-            const double D1 = zm + zz, D2 = zz + zp;
-            const double b1 = -asdq / D1, b2 = asdq / D2;
+            const double iD1 = 1.0 / (zm + zz), iD2 = 1.0 / (zz + zp);
+            const double b1 = -asdq * iD1, b2 = asdq * iD2;
             const double db1 = c0 * zm * bm_p - c0 * bm_t;
             const double db2 = c2 * zp * bp_p + c2 * bp_t;
             const double dcm = b1 * zm * bm_p - b1 * bm_t;
             const double dcp = b2 * zp * bp_p + b2 * bp_t;
-            const double dD1 = -b1 * db1 / D1, dD2 = -b2 * db2 / D2;
+            const double dD1 = -b1 * db1 * iD1, dD2 = -b2 * db2 * iD2;
             const double dzm = c0 * b1 * bm_p + dD1;
             const double dzp = c2 * b2 * bp_p + dD2;
             const double dzz = dD1 + dD2;
             g_r0 = c0 * dzm; g_c0 = rho0 * dzm + dcm;
             g_r1 = c1 * dzz; g_c1 = rho1 * dzz;
             g_r2 = c2 * dzp; g_c2 = rho2 * dzp + dcp;
-            return -db1 / D1 + db2 / D2;
+            return -db1 * iD1 + db2 * iD2;
         };
         gApd = split_T(Ap, LAp0, LAt0, LAp1, LAt1, LAp2, LAt2, oL, gA_r0, gA_c0, gA_r1, gA_c1, gA_r2, gA_c2);
         gPpd = split_T(Pp, LBp0, LBt0, LBp1, LBt1, LBp2, LBt2, oR, gB_r0, gB_c0, gB_r1, gB_c1, gB_r2, gB_c2);
@@ -261,14 +264,14 @@ __device__ __forceinline__ void adj_line(const AdjArgs& a, const double* __restr
         gW2p += phi2 * gL2p; gW2n += phi2 * gL2n;
         if (l1) {
             const double gr = dphi1 * (w1p * gL1p + w1n * gL1n);
-            const double gdot = gr / wn1, gwn = -r1 * gr / wn1;
+            const double gdot = gr / wn1, gwn = -r1 * gdot;   // a reciprocal of a denormal wn would overflow
             gW1p += 2.0 * gwn * w1p + gdot * nb1p;
             gW1n += 2.0 * gwn * w1n + gdot * nb1n;
             send1p = gdot * w1p; send1n = gdot * w1n;
         }
         if (l2) {
             const double gr = dphi2 * (w2p * gL2p + w2n * gL2n);
-            const double gdot = gr / wn2, gwn = -r2 * gr / wn2;
+            const double gdot = gr / wn2, gwn = -r2 * gdot;   // a reciprocal of a denormal wn would overflow
             gW2p += 2.0 * gwn * w2p + gdot * nb2p;
             gW2n += 2.0 * gwn * w2n + gdot * nb2n;
             send2p = gdot * w2p; send2n = gdot * w2n;
@@ -324,7 +327,7 @@ __device__ __forceinline__ void adj_line(const AdjArgs& a, const double* __restr
     o.ga_up[1] = gB_c2 + nup_c;
 }
 
-__global__ void __launch_bounds__(ANT, 1) adjoint_kernel(AdjArgs a)
+__global__ void __launch_bounds__(ANT, CLAW2_ADJ_MINB) adjoint_kernel(AdjArgs a)
 {
     __shared__ double GQ[3 * AR * AR];
     __shared__ double GA[2 * AR * AR];

@@ -69,8 +69,26 @@ def branch_ids(r, meth):
     return torch.where(0.0 > torch.where(1.0 < r, torch.ones_like(r), r), 0, torch.where(1.0 < r, 1, 2))
 
 
+class _Ratio(torch.autograd.Function):
+    """r = b / a with the derivative written as (g/a, -(g/a) r): torch's own
+    division backward forms b / (a*a), which underflows to a division by zero
+    when a (a squared wave norm) is subnormal."""
+
+    @staticmethod
+    def forward(ctx, b, a):
+        r = b / a
+        ctx.save_for_backward(a, r)
+        return r
+
+    @staticmethod
+    def backward(ctx, g):
+        a, r = ctx.saved_tensors
+        ga = g / a
+        return ga, -ga * r
+
+
 def philim(a, b, meth):
-    r = b / a
+    r = _Ratio.apply(b, a)
     if BRANCH_LOG is not None:
         BRANCH_LOG.append(branch_ids(r.detach(), meth))
     if meth == 4:
