@@ -139,6 +139,23 @@ def batched_vc_config(n=1024, seed=2024, nmin=64, nmax=384):
     return prob, insts
 
 
+def shallow_config(n=4096):
+    """Radial dam break: 4096^2 on [-2.5,2.5]^2, g = 1, h = 2 for r < 0.5 else 1,
+    hu = hv = 0; Roe with the transonic fix, superbee, unsplit with
+    transverse_waves=2, extrapolation BCs, cfl_desired 0.9.
+    Returns (problem, q0, run settings)."""
+    from pyclaw_b200 import _abi
+    x, dx = _centers(-2.5, 2.5, n)
+    y, dy = _centers(-2.5, 2.5, n)
+    X, Y = np.meshgrid(x, y, indexing="ij")
+    q = np.zeros((3, n, n), order="F")
+    q[0] = np.where(X ** 2 + Y ** 2 < 0.25, 2.0, 1.0)
+    prob = _abi.make_problem(rp=_abi.RP_SHALLOW_ROE, num_eqn=3, num_waves=3, num_aux=0, mx=n, my=n, dx=dx, dy=dy,
+                             order=2, transverse=2, mthlim=[2], params=(1.0,))
+    cmax = float(np.sqrt(2.0))
+    return prob, q, dict(cfl_max=1.0, cfl_desired=0.9, dt_initial=0.9 * dx / cmax)
+
+
 def adjoint_config(n=512, shots=64, nsteps=400, nrec=64, seed=7):
     """Seismic-style inversion workload on [-1,1]^2, surface at y = 1:
     variable-coefficient acoustics with a seeded target material (background
@@ -577,6 +594,78 @@ def run_batched(args):
     bs.close()
 
 
+def run_shallow(args):
+    """The 4096^2 shallow-water dam break: 500 controlled steps through the
+    device loop (claw2_advance), one CUDA-event pair around the whole run; the
+    state (403 MB per buffer) does not fit in L2, so nothing is flushed."""
+    import torch
+    from pyclaw_b200 import _abi, _lib
+    from pyclaw_b200.device import DeviceState
+    lib = _lib.load()
+    nsteps = args.sw_steps
+    prob, q, run = shallow_config(args.sw_n)
+    cells = prob.mx * prob.my
+    dev = DeviceState(prob, torch.device("cuda"))
+    host = _abi.Control.from_address(dev.ctrl_host.data_ptr())
+
+    def reset(max_steps):
+        dev.upload_q(q)
+        c = _abi.Control()
+        _lib.check(lib.claw2_control_init(ctypes.byref(c), 0.0, run["dt_initial"], 1e9, run["cfl_max"],
+                                          run["cfl_desired"], 1e99, 1, 0, int(max_steps), run["cfl_desired"]),
+                   "claw2_control_init")
+        ctypes.memmove(ctypes.addressof(host), ctypes.addressof(c), ctypes.sizeof(c))
+        dev.ctrl.copy_(dev.ctrl_host)
+        torch.cuda.synchronize()
+
+    def advance(n):
+        _lib.check(lib.claw2_advance(ctypes.byref(prob), dev.ptr(dev.q[0]), dev.ptr(dev.q[1]), dev.ptr(dev.aux),
+                                     dev.ptr(dev.ctrl), dev.ptr(dev.scratch), int(n), dev.stream), "claw2_advance")
+
+    reset(max(3, args.warmup))
+    advance(max(3, args.warmup))
+    reset(nsteps)
+    clocks = ClockSampler(torch.cuda.current_device())
+    clocks.start()
+    time.sleep(0.3)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    advance(nsteps)
+    e1.record()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    t = e0.elapsed_time(e1) / 1e3
+    dev.ctrl_host.copy_(dev.ctrl)
+    torch.cuda.synchronize()
+    # a fixed step count ends with the controller's max-steps status (the
+    # reference's "Maximum number of timesteps have been taken")
+    if host.error not in (0, _abi.ERR_MAX_STEPS) or host.iter != nsteps:
+        raise RuntimeError("device loop error %d after %d steps" % (host.error, host.iter))
+    acc = host.numsteps
+    value = acc * cells / t
+    peak, peak_kind = _peaks()
+    alg = 8 * 2 * prob.num_eqn * cells
+    achieved = alg / (t / nsteps) / 1e9
+    cpu = None
+    if not args.no_cpu:
+        rate, n, thr, el = cpu_rate(prob, q, run, omp=True, max_seconds=10.0)
+        cpu = {"value": rate, "unit": "cell-updates/s", "cores": thr, "kind": "port",
+               "sample": "%d whole-grid steps (%.1f s) of the 4096^2 dam break, oracle OpenMP gather form, "
+                         "%d threads" % (n, el, thr)}
+    line = {
+        "metric": "cell_updates_per_s", "value": value, "unit": "cell-updates/s", "n_gpus": 1,
+        "steps": nsteps, "ms_per_step": t / nsteps * 1e3, "higher_is_better": True, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": "shallow_water_dam_break_%dx%d" % (prob.mx, prob.my), "solver": "shallow_roe_efix",
+                   "limiter": "superbee", "transverse_waves": 2, "accepted_steps": int(acc),
+                   "t_final": host.t, "l2": "state (%d MB per buffer) larger than L2" % (8 * 3 * cells >> 20)},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None, "peak_kind": peak_kind},
+        "clocks": clk, "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def run_adjoint(args):
     """The adjoint workload: traces of `shots` shots over `nsteps` steps for the
     starting material, the L2 misfit against the target material's traces,
@@ -660,7 +749,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--workload", default="shockbubble", choices=["shockbubble", "batched", "adjoint"])
+    ap.add_argument("--workload", default="shockbubble", choices=["shockbubble", "batched", "adjoint", "shallow"])
+    ap.add_argument("--sw-n", type=int, default=4096)
+    ap.add_argument("--sw-steps", type=int, default=500)
     ap.add_argument("--instances", type=int, default=1024)
     ap.add_argument("--adj-n", type=int, default=512)
     ap.add_argument("--adj-shots", type=int, default=64)
@@ -674,6 +765,9 @@ def main():
         elif args.workload == "adjoint":
             if rank == 0:
                 run_adjoint(args)
+        elif args.workload == "shallow":
+            if rank == 0:
+                run_shallow(args)
         elif args.impl == "reference":
             run_reference_arm(args, world, rank)
         else:
