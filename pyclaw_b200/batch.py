@@ -198,7 +198,12 @@ class BatchSolver(object):
         nv = self.lib.claw2_batch_num_variants()
         times = {}
         for v in range(nv):
-            self.advance(1, v)                       # configure + warm
+            try:
+                self.advance(1, v)                   # configure + warm
+            except _lib.ClawStatusError as e:
+                if e.code == _abi.ERR_UNSUPPORTED:   # a launch shape this solver does not have
+                    continue
+                raise
             torch.cuda.synchronize(self.device)
             best = float("inf")
             for _ in range(repeats):

@@ -2,8 +2,8 @@
 // hand-written adjoint of its unsplit step (include/claw2_adjoint.h).
 //
 // Forward.  A shot is one wavefield; all shots share aux = (rho, c) and dt.
-// claw2_shots_step runs the fused tile step of claw2_kernels.cuh with the
-// shot as the third grid dimension.
+// claw2_shots_step runs the fused tile step (the light body of
+// claw2_light.cuh) with the shot as the third grid dimension.
 //
 // Adjoint.  One step of the reference's unsplit method (step2.f90:92-248,
 // flux2.f90:104-206, limiter.f90:34-58, philim.f90:18-55) with the vc-acoustics
@@ -35,6 +35,7 @@
 #include "../../include/claw2.h"
 #include "../../include/claw2_adjoint.h"
 #include "claw2_kernels.cuh"
+#include "claw2_light.cuh"
 
 namespace claw2 {
 namespace adj {
@@ -436,7 +437,10 @@ __global__ void __launch_bounds__(ANT, CLAW2_ADJ_MINB) adjoint_kernel(AdjArgs a)
 // ---------------------------------------------------------------------------
 // forward: the plain tile step with the shot as third grid dimension
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256, 2) shots_step_kernel(StepArgs common, long long qstride)
+#ifndef CLAW2_LIGHT_MINB
+#define CLAW2_LIGHT_MINB 3
+#endif
+__global__ void __launch_bounds__(256, CLAW2_LIGHT_MINB) shots_step_kernel(StepArgs common, long long qstride)
 {
     extern __shared__ double smem_dyn[];
     DevCtx ctx{smem_dyn};
@@ -449,7 +453,7 @@ __global__ void __launch_bounds__(256, 2) shots_step_kernel(StepArgs common, lon
     a.cfl_out += shot;
     const TileId t{(int)blockIdx.x, (int)blockIdx.y, (int)gridDim.x, (int)gridDim.y,
                    (int)(blockIdx.y * gridDim.x + blockIdx.x), (int)(gridDim.x * gridDim.y)};
-    step_tile_at<RpVcAcoustics, FT, FT, 256, false>(a, ctx, t);
+    light_tile_at<RpVcAcoustics, FT, FT, 256>(a, ctx, t);
 }
 
 struct ShotIO {
@@ -627,7 +631,7 @@ int claw2_shots_step(const claw2_problem* p, int nshots, long long shot_stride, 
     a.ticket = static_cast<unsigned int*>(scratch);
     a.partials = reinterpret_cast<double*>(static_cast<char*>(scratch) + tickets);
     a.cfl_out = cfl_dev;
-    using SM = TileSmem<RpVcAcoustics, FT, FT, 256, false>;
+    using SM = LightSmem<FT, FT, 256>;
     static bool configured = false;
     if (!configured) {
         if (cudaFuncSetAttribute(shots_step_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SM::bytes) !=

@@ -14,6 +14,7 @@
 #define CLAW2_EXPORT __attribute__((visibility("default")))
 #include "../../include/claw2.h"
 #include "claw2_kernels.cuh"
+#include "claw2_light.cuh"
 
 namespace claw2 {
 
@@ -29,9 +30,29 @@ __global__ void __launch_bounds__(NT, CLAW2_MINB) step_kernel(StepArgs a)
     step_tile<RP, TX, TY, NT, SPLIT>(a, ctx);
 }
 
+// The two-wave acoustics solvers have a leaner unsplit body (claw2_light.cuh)
+// that needs fewer registers and less shared memory, so more CTAs fit per SM.
+template <class RP> struct HasLight { static constexpr bool value = false; };
+template <> struct HasLight<RpAcoustics> { static constexpr bool value = true; };
+template <> struct HasLight<RpVcAcoustics> { static constexpr bool value = true; };
+
+#ifndef CLAW2_LIGHT_MINB
+#define CLAW2_LIGHT_MINB 3
+#endif
+
+template <class RP>
+__global__ void __launch_bounds__(256, CLAW2_LIGHT_MINB) light_step_kernel(StepArgs a)
+{
+    extern __shared__ double smem_dyn[];
+    DevCtx ctx{smem_dyn};
+    const TileId t{(int)blockIdx.x, (int)blockIdx.y, (int)gridDim.x, (int)gridDim.y,
+                   (int)(blockIdx.y * gridDim.x + blockIdx.x), (int)(gridDim.x * gridDim.y)};
+    light_tile_at<RP, 29, 29, 256>(a, ctx, t);
+}
+
 // Batched step: a persistent grid walks the concatenated tile list of all
 // instances; each tile is one step_tile_at call with that instance's buffers.
-template <class RP, int NT, int MINB>
+template <class RP, int NT, int MINB, bool LIGHT>
 __global__ void __launch_bounds__(NT, MINB)
 batch_kernel(const claw2_batch_instance* __restrict__ inst, int ninst, int ntiles, StepArgs common)
 {
@@ -52,7 +73,8 @@ batch_kernel(const claw2_batch_instance* __restrict__ inst, int ninst, int ntile
         a.ghost_fused = (I.mx >= 4 && I.my >= 4) ? common.ghost_fused : 0;
         const int lt = t - I.tile_begin;
         const TileId tile{lt % I.nbx, lt / I.nbx, I.nbx, I.nby, lt, I.nbx * I.nby};
-        step_tile_at<RP, 29, 29, NT, false>(a, ctx, tile);
+        if constexpr (LIGHT) light_tile_at<RP, 29, 29, NT>(a, ctx, tile);
+        else step_tile_at<RP, 29, 29, NT, false>(a, ctx, tile);
         __syncthreads();                            // shared memory is reused by the next tile
     }
 }
@@ -222,9 +244,26 @@ void fill_args(const claw2_problem* p, double* q, StepArgs& a)
     (void)q;
 }
 
+template <class RP>
+int launch_light(const StepArgs& a, int nbx, int nby, cudaStream_t st)
+{
+    using SM = LightSmem<29, 29, 256>;
+    auto kern = light_step_kernel<RP>;
+    static bool configured = false;
+    if (!configured) {
+        if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SM::bytes) != cudaSuccess)
+            return CLAW2_ERR_CUDA;
+        configured = true;
+    }
+    kern<<<dim3(nbx, nby), 256, SM::bytes, st>>>(a);
+    return cudaGetLastError() == cudaSuccess ? CLAW2_OK : CLAW2_ERR_CUDA;
+}
+
 template <class RP, bool SPLIT>
 int launch_step_t(const StepArgs& a, int nbx, int nby, cudaStream_t st)
 {
+    if constexpr (!SPLIT && HasLight<RP>::value)
+        if (a.capa < 0 && !a.fwave) return launch_light<RP>(a, nbx, nby, st);
     constexpr int TX = SPLIT ? STX : UTX, TY = SPLIT ? STY : UTY, NT = SPLIT ? SNT : UNT;
     using SM = TileSmem<RP, TX, TY, NT, SPLIT>;
     auto kern = step_kernel<RP, TX, TY, NT, SPLIT>;
@@ -472,29 +511,31 @@ int claw2_device_to_ref(const claw2_problem* p, int ncomp, const double* dev, do
 
 namespace {
 struct BatchVariant { int threads, minb; };
-constexpr BatchVariant kBatchVariants[] = {{256, 2}, {128, 4}, {128, 3}, {512, 1}};
+// the last two exist for the light body only (claw2_batch_advance returns
+// CLAW2_ERR_UNSUPPORTED for them with the other solvers)
+constexpr BatchVariant kBatchVariants[] = {{256, 2}, {128, 4}, {128, 3}, {512, 1}, {256, 3}, {256, 4}};
 constexpr int kNumBatchVariants = sizeof(kBatchVariants) / sizeof(kBatchVariants[0]);
 
-template <class RP, int NT, int MINB>
+template <class RP, int NT, int MINB, bool LIGHT>
 int batch_launch_t(const StepArgs& common, const claw2_batch_instance* inst, int ninst, int ntiles, int nsteps,
                    cudaStream_t st)
 {
-    using SM = TileSmem<RP, 29, 29, NT, false>;
-    auto kern = batch_kernel<RP, NT, MINB>;
+    constexpr int SMB = LIGHT ? LightSmem<29, 29, NT>::bytes : TileSmem<RP, 29, 29, NT, false>::bytes;
+    auto kern = batch_kernel<RP, NT, MINB, LIGHT>;
     static int grid = 0;
     if (grid == 0) {
-        if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SM::bytes) != cudaSuccess)
+        if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SMB) != cudaSuccess)
             return CLAW2_ERR_CUDA;
         int dev = 0, nsm = 0, occ = 0;
         if (cudaGetDevice(&dev) != cudaSuccess ||
             cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, NT, SM::bytes) != cudaSuccess || occ < 1)
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, NT, SMB) != cudaSuccess || occ < 1)
             return CLAW2_ERR_CUDA;
         grid = nsm * occ;
     }
     const int g = ntiles < grid ? ntiles : grid;
     for (int n = 0; n < nsteps; n++) {
-        kern<<<g, NT, SM::bytes, st>>>(inst, ninst, ntiles, common);
+        kern<<<g, NT, SMB, st>>>(inst, ninst, ntiles, common);
         if (cudaGetLastError() != cudaSuccess) return CLAW2_ERR_CUDA;
     }
     return CLAW2_OK;
@@ -504,11 +545,25 @@ template <class RP>
 int batch_launch_rp(int variant, const StepArgs& c, const claw2_batch_instance* inst, int ninst, int ntiles,
                     int nsteps, cudaStream_t st)
 {
+    if constexpr (HasLight<RP>::value) {
+        if (c.capa < 0 && !c.fwave) {
+            switch (variant) {
+            case 0: return batch_launch_t<RP, 256, 2, true>(c, inst, ninst, ntiles, nsteps, st);
+            case 1: return batch_launch_t<RP, 128, 4, true>(c, inst, ninst, ntiles, nsteps, st);
+            case 2: return batch_launch_t<RP, 128, 3, true>(c, inst, ninst, ntiles, nsteps, st);
+            case 3: return batch_launch_t<RP, 512, 1, true>(c, inst, ninst, ntiles, nsteps, st);
+            case 4: return batch_launch_t<RP, 256, 3, true>(c, inst, ninst, ntiles, nsteps, st);
+            case 5: return batch_launch_t<RP, 256, 4, true>(c, inst, ninst, ntiles, nsteps, st);
+            default: return CLAW2_ERR_INVALID;
+            }
+        }
+    }
     switch (variant) {
-    case 0: return batch_launch_t<RP, 256, 2>(c, inst, ninst, ntiles, nsteps, st);
-    case 1: return batch_launch_t<RP, 128, 4>(c, inst, ninst, ntiles, nsteps, st);
-    case 2: return batch_launch_t<RP, 128, 3>(c, inst, ninst, ntiles, nsteps, st);
-    case 3: return batch_launch_t<RP, 512, 1>(c, inst, ninst, ntiles, nsteps, st);
+    case 0: return batch_launch_t<RP, 256, 2, false>(c, inst, ninst, ntiles, nsteps, st);
+    case 1: return batch_launch_t<RP, 128, 4, false>(c, inst, ninst, ntiles, nsteps, st);
+    case 2: return batch_launch_t<RP, 128, 3, false>(c, inst, ninst, ntiles, nsteps, st);
+    case 3: return batch_launch_t<RP, 512, 1, false>(c, inst, ninst, ntiles, nsteps, st);
+    case 4: case 5: return CLAW2_ERR_UNSUPPORTED;
     default: return CLAW2_ERR_INVALID;
     }
 }

@@ -515,6 +515,61 @@ struct TileId {
     int bx, by, nbx, nby, part, ntiles;
 };
 
+// Final values of the tile's cells (Qx: row stride TX, component stride QSTR,
+// row 0 = tile row j0) and their ghost images, then the block CFL max and the
+// last-arriving CTA's reduction over all CTAs (and, in controlled mode, the
+// device-side time-step controller).
+template <int MEQN, int TX, int TY, int NT, class Ctx>
+CLAW2_HD void finish_tile(const StepArgs& a, Ctx& ctx, const TileId& tile, const double* Qx, int QSTR, double* red,
+                          double* qout, int i0, int j0, double cflm)
+{
+    const int tid = ctx.tid();
+    int bad = 0;
+    for (int idx = tid; idx < TX * TY; idx += NT) {
+        const int ci = idx % TX, cj = idx / TX;
+        const int i = i0 + ci, j = j0 + cj;
+        if (i >= a.mx || j >= a.my) continue;
+        double v[MEQN];
+#pragma unroll
+        for (int m = 0; m < MEQN; m++) {
+            v[m] = Qx[m * QSTR + cj * TX + ci];
+            if (!isfinite(v[m])) bad = 1;
+        }
+        write_cell<MEQN>(a, qout, i, j, v);
+    }
+
+    // ---- block CFL max (deterministic: max is exact) and last-block epilogue
+    red[tid] = bad ? -1.0 : cflm;        // CFL numbers are >= 0; -1 flags a non-finite cell
+    ctx.sync();
+    if (tid == 0) {
+        double mxv = 0.0;
+        int nf = 0;
+        for (int t = 0; t < NT; t++) {
+            if (red[t] < 0.0) nf = 1;
+            else mxv = mxv > red[t] ? mxv : red[t];
+        }
+        const int nblocks = tile.ntiles;
+        const int bid = tile.part;
+        a.partials[bid] = nf ? -1.0 : mxv;
+        ctx.fence();
+        const unsigned int prev = ctx.atomic_inc(a.ticket);
+        if (prev == (unsigned int)(nblocks - 1)) {
+            ctx.fence();
+            double cfl = 0.0;
+            int nonfinite = 0;
+            for (int b = 0; b < nblocks; b++) {
+                const double v = ctx.load_volatile(&a.partials[b]);
+                if (v < 0.0) nonfinite = 1;
+                else cfl = cfl > v ? cfl : v;
+            }
+            if (a.ctrl) control_update(a.ctrl, cfl, nonfinite);
+            else *a.cfl_out = nonfinite ? ctx.nan() : cfl;
+            *a.ticket = 0u;
+            ctx.fence();
+        }
+    }
+}
+
 template <class RP, int TX, int TY, int NT, bool SPLIT, class Ctx>
 CLAW2_HD void step_tile_at(const StepArgs& a, Ctx& ctx, const TileId& tile)
 {
@@ -593,51 +648,7 @@ CLAW2_HD void step_tile_at(const StepArgs& a, Ctx& ctx, const TileId& tile)
         }
     }
 
-    // ---- final values of the tile's cells and their ghost images
-    int bad = 0;
-    for (int idx = tid; idx < TX * TY; idx += NT) {
-        const int ci = idx % TX, cj = idx / TX;
-        const int i = i0 + ci, j = j0 + cj;
-        if (i >= a.mx || j >= a.my) continue;
-        double v[MEQN];
-#pragma unroll
-        for (int m = 0; m < MEQN; m++) {
-            v[m] = Qx[(m * QROWS + (cj - QROW0)) * TX + ci];
-            if (!isfinite(v[m])) bad = 1;
-        }
-        write_cell<MEQN>(a, qout, i, j, v);
-    }
-
-    // ---- block CFL max (deterministic: max is exact) and last-block epilogue
-    red[tid] = bad ? -1.0 : cflm;        // CFL numbers are >= 0; -1 flags a non-finite cell
-    ctx.sync();
-    if (tid == 0) {
-        double mxv = 0.0;
-        int nf = 0;
-        for (int t = 0; t < NT; t++) {
-            if (red[t] < 0.0) nf = 1;
-            else mxv = mxv > red[t] ? mxv : red[t];
-        }
-        const int nblocks = tile.ntiles;
-        const int bid = tile.part;
-        a.partials[bid] = nf ? -1.0 : mxv;
-        ctx.fence();
-        const unsigned int prev = ctx.atomic_inc(a.ticket);
-        if (prev == (unsigned int)(nblocks - 1)) {
-            ctx.fence();
-            double cfl = 0.0;
-            int nonfinite = 0;
-            for (int b = 0; b < nblocks; b++) {
-                const double v = ctx.load_volatile(&a.partials[b]);
-                if (v < 0.0) nonfinite = 1;
-                else cfl = cfl > v ? cfl : v;
-            }
-            if (a.ctrl) control_update(a.ctrl, cfl, nonfinite);
-            else *a.cfl_out = nonfinite ? ctx.nan() : cfl;
-            *a.ticket = 0u;
-            ctx.fence();
-        }
-    }
+    finish_tile<MEQN, TX, TY, NT>(a, ctx, tile, Qx + (-QROW0) * TX, QROWS * TX, red, qout, i0, j0, cflm);
 }
 
 template <class RP, int TX, int TY, int NT, bool SPLIT, class Ctx>
@@ -665,6 +676,9 @@ struct DevCtx {
     __device__ __forceinline__ double load_volatile(const double* p) const { return *(volatile const double*)p; }
     __device__ __forceinline__ double nan() const { return __longlong_as_double(0x7ff8000000000000ULL); }
     __device__ __forceinline__ double* smem() const { return sm; }
+    // value of the lane below / above in the warp (own value at the ends)
+    __device__ __forceinline__ double shfl_up(double v) const { return __shfl_up_sync(0xffffffffu, v, 1); }
+    __device__ __forceinline__ double shfl_down(double v) const { return __shfl_down_sync(0xffffffffu, v, 1); }
 };
 #endif
 
