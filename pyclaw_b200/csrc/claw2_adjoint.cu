@@ -113,10 +113,39 @@ struct LineOut {
     double ga_own[2], ga_dn[2], ga_up[2];
 };
 
+// Transposed transverse split of a fluctuation with pressure component `asdq`
+// sitting in a cell whose (rho, c) on the lines below/at/above are
+// (r0,c0)/(r1,c1)/(r2,c2) and whose impedance-sum reciprocals are iD1 =
+// 1/(z0+z1), iD2 = 1/(z1+z2).  bm_*, bp_*: adjoints of bmasdq/bpasdq
+// (pressure and transverse components).  Returns d/d asdq; g_*: aux gradient.
+__device__ __forceinline__ double split_T(double asdq, double bm_p, double bm_t, double bp_p, double bp_t, double r0,
+                                          double c0, double r1, double c1, double r2, double c2, double iD1,
+                                          double iD2, double& gr0, double& gc0, double& gr1, double& gc1,
+                                          double& gr2, double& gc2)
+{
+    const double zm = r0 * c0, zp = r2 * c2;
+    const double b1 = -asdq * iD1, b2 = asdq * iD2;
+    const double db1 = c0 * zm * bm_p - c0 * bm_t;
+    const double db2 = c2 * zp * bp_p + c2 * bp_t;
+    const double dcm = b1 * zm * bm_p - b1 * bm_t;
+    const double dcp = b2 * zp * bp_p + b2 * bp_t;
+    const double dD1 = -b1 * db1 * iD1, dD2 = -b2 * db2 * iD2;
+    const double dzm = c0 * b1 * bm_p + dD1;
+    const double dzp = c2 * b2 * bp_p + dD2;
+    const double dzz = dD1 + dD2;
+    gr0 = c0 * dzm; gc0 = r0 * dzm + dcm;
+    gr1 = c1 * dzz; gc1 = r1 * dzz;
+    gr2 = c2 * dzp; gc2 = r2 * dzp + dcp;
+    return -db1 * iD1 + db2 * iD2;
+}
+
+// One slice line of the adjoint.  full = false for a line whose cells the
+// tile does not own: only its transverse splits' aux gradients on the
+// neighbouring lines (ga_dn, ga_up) are needed.
 template <int IXY>
 __device__ __forceinline__ void adj_line(const AdjArgs& a, const double* __restrict__ q,
                                          const double* __restrict__ lin, int i0, int j0, int line, bool lineok,
-                                         LineOut& o)
+                                         bool full, LineOut& o)
 {
     constexpr int MN = IXY == 1 ? 1 : 2;     // normal velocity component
     constexpr int MT = IXY == 1 ? 2 : 1;     // transverse velocity component
@@ -131,6 +160,7 @@ __device__ __forceinline__ void adj_line(const AdjArgs& a, const double* __restr
     // the forward solves interfaces -1..len+1 of slices -1..len_other and limits 0..len
     const bool ex = lineok && k >= -1 && k <= len + 1;
     const bool lim = ex && a.order == 2 && k >= 0 && k <= len && lane >= 1 && lane <= 30;
+    const bool trans = a.trans > 0;
     const long long oR = IXY == 1 ? cell(a, k, line) : cell(a, line, k);
     const long long oL = oR - along;
 
@@ -149,14 +179,12 @@ __device__ __forceinline__ void adj_line(const AdjArgs& a, const double* __restr
     }
     const double w1p = -a1 * zL, w1n = a1, w2p = a2 * zR, w2n = a2;
     const double s1 = -cL, s2 = cR;
-
-    // neighbours' waves (interfaces k-1 and k+1)
     const double w1p_l = __shfl_up_sync(FULL, w1p, 1), w1n_l = __shfl_up_sync(FULL, w1n, 1);
     const double w2p_l = __shfl_up_sync(FULL, w2p, 1), w2n_l = __shfl_up_sync(FULL, w2n, 1);
     const double w1p_r = __shfl_down_sync(FULL, w1p, 1), w1n_r = __shfl_down_sync(FULL, w1n, 1);
     const double w2p_r = __shfl_down_sync(FULL, w2p, 1), w2n_r = __shfl_down_sync(FULL, w2n, 1);
 
-    // ---------------- forward recompute: limiter ----------------
+    // ---------------- forward recompute: limiter and corrections ----------------
     bool l1 = false, l2 = false;
     double phi1 = 1.0, phi2 = 1.0, dphi1 = 0.0, dphi2 = 0.0, r1 = 0.0, r2 = 0.0, wn1 = 1.0, wn2 = 1.0;
     double nb1p = 0.0, nb1n = 0.0, nb2p = 0.0, nb2n = 0.0;
@@ -183,167 +211,210 @@ __device__ __forceinline__ void adj_line(const AdjArgs& a, const double* __restr
         }
     }
     const bool second = a.order == 2;
+    const bool cor = second && a.trans == 2;
     const double dtave = 0.5 * (dtn + dtn);
     const double as1 = fabs(s1), as2 = fabs(s2);
     const double f1 = as1 * (1.0 - as1 * dtave), f2 = as2 * (1.0 - as2 * dtave);
-    const double L1p = phi1 * w1p, L1n = phi1 * w1n, L2p = phi2 * w2p, L2n = phi2 * w2n;
-    const double cqp = second ? f1 * L1p + f2 * L2p : 0.0;
-    const bool cor = second && a.trans == 2;
-    const double Ap = s1 * w1p + (cor ? cqp : 0.0);     // asdq(1) of the two transverse splits
-    const double Pp = s2 * w2p - (cor ? cqp : 0.0);
+    const double cqp = second ? f1 * (phi1 * w1p) + f2 * (phi2 * w2p) : 0.0;
 
-    // ---------------- adjoint of the update: the interface's outputs ----------------
-    // lambda at cells k-1 (A) and k (B) on the line and the lines below/above
-    double LAp0 = 0, LAt0 = 0, LAp1 = 0, LAn1 = 0, LAt1 = 0, LAp2 = 0, LAt2 = 0;
-    double LBp0 = 0, LBt0 = 0, LBp1 = 0, LBn1 = 0, LBt1 = 0, LBp2 = 0, LBt2 = 0;
-    if (ex) {
-        LAp1 = lin[oL]; LAn1 = lin[oL + MN * P]; LAt1 = lin[oL + MT * P];
-        LBp1 = lin[oR]; LBn1 = lin[oR + MN * P]; LBt1 = lin[oR + MT * P];
-        if (a.trans > 0) {
-            LAp0 = lin[oL - across]; LAt0 = lin[oL - across + MT * P];
-            LAp2 = lin[oL + across]; LAt2 = lin[oL + across + MT * P];
-            LBp0 = lin[oR - across]; LBt0 = lin[oR - across + MT * P];
-            LBp2 = lin[oR + across]; LBt2 = lin[oR + across + MT * P];
-        }
+    // ---------------- transverse splits, transposed ----------------
+    // this lane's cell k on the lines below/above, and the impedance-sum
+    // reciprocals of cell k (cell k-1's come from the lane to the left)
+    double rB0 = 0.0, cB0 = 0.0, rB2 = 0.0, cB2 = 0.0, iB1 = 0.0, iB2 = 0.0;
+    if (ex && trans) {
+        rB0 = aux[oR - across]; cB0 = aux[oR - across + P];
+        rB2 = aux[oR + across]; cB2 = aux[oR + across + P];
+        iB1 = 1.0 / (rB0 * cB0 + zR);
+        iB2 = 1.0 / (zR + rB2 * cB2);
     }
-    double gAm_p = -dtn * LAp1, gAm_n = -dtn * LAn1;            // d/d amdq
-    double gAp_p = -dtn * LBp1, gAp_n = -dtn * LBn1;            // d/d apdq
-    const double gF_p = -dtn * (LAp1 - LBp1), gF_n = -dtn * (LAn1 - LBn1);   // d/d fadd
-
-    // ---------------- transverse splits (RpVcAcoustics::rpt2), transposed ----------------
-    // aux gradient of cell k-1 (A) and cell k (B) on lines -1, 0, +1
+    const double iA1 = __shfl_up_sync(FULL, iB1, 1), iA2 = __shfl_up_sync(FULL, iB2, 1);
     double gA_r0 = 0, gA_c0 = 0, gA_r1 = 0, gA_c1 = 0, gA_r2 = 0, gA_c2 = 0;
     double gB_r0 = 0, gB_c0 = 0, gB_r1 = 0, gB_c1 = 0, gB_r2 = 0, gB_c2 = 0;
-    double gApd = 0.0, gPpd = 0.0;                               // d/d asdq(1)
-    if (ex && a.trans > 0) {
+    double gApd = 0.0, gPpd = 0.0;                                // d/d asdq(1) of A and P
+    if (ex && trans) {
         const double h = 0.5 * dtn;
-        // g1(c) = dtt (lam(c) - lam(c, below)), g2(c) = dtt (lam(c, above) - lam(c))
-        auto split_T = [&](double asdq, double lp0, double lt0, double lp1, double lt1, double lp2, double lt2,
-                           long long oc, double& g_r0, double& g_c0, double& g_r1, double& g_c1, double& g_r2,
-                           double& g_c2) -> double {
-            const double bm_p = -h * (dtt * (lp1 - lp0)), bm_t = -h * (dtt * (lt1 - lt0));   // d/d bmasdq
-            const double bp_p = -h * (dtt * (lp2 - lp1)), bp_t = -h * (dtt * (lt2 - lt1));   // d/d bpasdq
-            const double rho0 = aux[oc - across], c0 = aux[oc - across + P];
-            const double rho1 = aux[oc], c1 = aux[oc + P];
-            const double rho2 = aux[oc + across], c2 = aux[oc + across + P];
-            const double zm = rho0 * c0, zz = rho1 * c1, zp = rho2 * c2;
-            const double iD1 = 1.0 / (zm + zz), iD2 = 1.0 / (zz + zp);
-            const double b1 = -asdq * iD1, b2 = asdq * iD2;
-            const double db1 = c0 * zm * bm_p - c0 * bm_t;
-            const double db2 = c2 * zp * bp_p + c2 * bp_t;
-            const double dcm = b1 * zm * bm_p - b1 * bm_t;
-            const double dcp = b2 * zp * bp_p + b2 * bp_t;
-            const double dD1 = -b1 * db1 * iD1, dD2 = -b2 * db2 * iD2;
-            const double dzm = c0 * b1 * bm_p + dD1;
-            const double dzp = c2 * b2 * bp_p + dD2;
-            const double dzz = dD1 + dD2;
-            g_r0 = c0 * dzm; g_c0 = rho0 * dzm + dcm;
-            g_r1 = c1 * dzz; g_c1 = rho1 * dzz;
-            g_r2 = c2 * dzp; g_c2 = rho2 * dzp + dcp;
-            return -db1 * iD1 + db2 * iD2;
-        };
-        gApd = split_T(Ap, LAp0, LAt0, LAp1, LAt1, LAp2, LAt2, oL, gA_r0, gA_c0, gA_r1, gA_c1, gA_r2, gA_c2);
-        gPpd = split_T(Pp, LBp0, LBt0, LBp1, LBt1, LBp2, LBt2, oR, gB_r0, gB_c0, gB_r1, gB_c1, gB_r2, gB_c2);
+        const double LAp0 = lin[oL - across], LAt0 = lin[oL - across + MT * P];
+        const double LAp1 = lin[oL], LAt1 = lin[oL + MT * P];
+        const double LAp2 = lin[oL + across], LAt2 = lin[oL + across + MT * P];
+        const double LBp0 = lin[oR - across], LBt0 = lin[oR - across + MT * P];
+        const double LBp1 = lin[oR], LBt1 = lin[oR + MT * P];
+        const double LBp2 = lin[oR + across], LBt2 = lin[oR + across + MT * P];
+        const double Ap = s1 * w1p + (cor ? cqp : 0.0);
+        const double Pp = s2 * w2p - (cor ? cqp : 0.0);
+        const double rA0 = aux[oL - across], cA0 = aux[oL - across + P];
+        const double rA2 = aux[oL + across], cA2 = aux[oL + across + P];
+        // g1(c) = dtt (lam(c) - lam(c, below)), g2(c) = dtt (lam(c, above) - lam(c)); d/d bm = -h g1, d/d bp = -h g2
+        gApd = split_T(Ap, -h * (dtt * (LAp1 - LAp0)), -h * (dtt * (LAt1 - LAt0)), -h * (dtt * (LAp2 - LAp1)),
+                       -h * (dtt * (LAt2 - LAt1)), rA0, cA0, rhoL, cL, rA2, cA2, iA1, iA2, gA_r0, gA_c0, gA_r1, gA_c1,
+                       gA_r2, gA_c2);
+        gPpd = split_T(Pp, -h * (dtt * (LBp1 - LBp0)), -h * (dtt * (LBt1 - LBt0)), -h * (dtt * (LBp2 - LBp1)),
+                       -h * (dtt * (LBt2 - LBt1)), rB0, cB0, rhoR, cR, rB2, cB2, iB1, iB2, gB_r0, gB_c0, gB_r1, gB_c1,
+                       gB_r2, gB_c2);
     }
-    gAm_p += gApd;
-    gAp_p += gPpd;
 
     // ---------------- correction fluxes and limiter, transposed ----------------
-    double gW1p = s1 * gAm_p, gW1n = s1 * gAm_n, gW2p = s2 * gAp_p, gW2n = s2 * gAp_n;
-    double gs1 = w1p * gAm_p + w1n * gAm_n, gs2 = w2p * gAp_p + w2n * gAp_n;
+    double gW1p = 0, gW1n = 0, gW2p = 0, gW2n = 0, gs1 = 0, gs2 = 0;
     double send1p = 0.0, send1n = 0.0, send2p = 0.0, send2n = 0.0;   // to the upwind neighbour's wave
-    if (ex && second) {
-        const double gcq_p = 0.5 * gF_p + (cor ? gApd - gPpd : 0.0);
-        const double gcq_n = 0.5 * gF_n;
-        const double gL1p = f1 * gcq_p, gL1n = f1 * gcq_n, gL2p = f2 * gcq_p, gL2n = f2 * gcq_n;
-        const double gf1 = L1p * gcq_p + L1n * gcq_n, gf2 = L2p * gcq_p + L2n * gcq_n;
-        const double sg1 = s1 > 0.0 ? 1.0 : (s1 < 0.0 ? -1.0 : 0.0);
-        const double sg2 = s2 > 0.0 ? 1.0 : (s2 < 0.0 ? -1.0 : 0.0);
-        gs1 += sg1 * (1.0 - 2.0 * as1 * dtave) * gf1;
-        gs2 += sg2 * (1.0 - 2.0 * as2 * dtave) * gf2;
-        gW1p += phi1 * gL1p; gW1n += phi1 * gL1n;
-        gW2p += phi2 * gL2p; gW2n += phi2 * gL2n;
-        if (l1) {
-            const double gr = dphi1 * (w1p * gL1p + w1n * gL1n);
-            const double gdot = gr / wn1, gwn = -r1 * gdot;   // a reciprocal of a denormal wn would overflow
-            gW1p += 2.0 * gwn * w1p + gdot * nb1p;
-            gW1n += 2.0 * gwn * w1n + gdot * nb1n;
-            send1p = gdot * w1p; send1n = gdot * w1n;
-        }
-        if (l2) {
-            const double gr = dphi2 * (w2p * gL2p + w2n * gL2n);
-            const double gdot = gr / wn2, gwn = -r2 * gdot;   // a reciprocal of a denormal wn would overflow
-            gW2p += 2.0 * gwn * w2p + gdot * nb2p;
-            gW2n += 2.0 * gwn * w2n + gdot * nb2n;
-            send2p = gdot * w2p; send2n = gdot * w2n;
+    if (full && ex) {
+        const double LAp1 = lin[oL], LAn1 = lin[oL + MN * P];
+        const double LBp1 = lin[oR], LBn1 = lin[oR + MN * P];
+        const double gAm_p = -dtn * LAp1 + gApd, gAm_n = -dtn * LAn1;   // d/d amdq
+        const double gAp_p = -dtn * LBp1 + gPpd, gAp_n = -dtn * LBn1;   // d/d apdq
+        gW1p = s1 * gAm_p; gW1n = s1 * gAm_n; gW2p = s2 * gAp_p; gW2n = s2 * gAp_n;
+        gs1 = w1p * gAm_p + w1n * gAm_n;
+        gs2 = w2p * gAp_p + w2n * gAp_n;
+        if (second) {
+            const double gcq_p = 0.5 * (-dtn * (LAp1 - LBp1)) + (cor ? gApd - gPpd : 0.0);
+            const double gcq_n = 0.5 * (-dtn * (LAn1 - LBn1));
+            const double gL1p = f1 * gcq_p, gL1n = f1 * gcq_n, gL2p = f2 * gcq_p, gL2n = f2 * gcq_n;
+            const double gf1 = phi1 * (w1p * gcq_p + w1n * gcq_n), gf2 = phi2 * (w2p * gcq_p + w2n * gcq_n);
+            const double sg1 = s1 > 0.0 ? 1.0 : (s1 < 0.0 ? -1.0 : 0.0);
+            const double sg2 = s2 > 0.0 ? 1.0 : (s2 < 0.0 ? -1.0 : 0.0);
+            gs1 += sg1 * (1.0 - 2.0 * as1 * dtave) * gf1;
+            gs2 += sg2 * (1.0 - 2.0 * as2 * dtave) * gf2;
+            gW1p += phi1 * gL1p; gW1n += phi1 * gL1n;
+            gW2p += phi2 * gL2p; gW2n += phi2 * gL2n;
+            if (l1) {
+                const double gr = dphi1 * (w1p * gL1p + w1n * gL1n);
+                const double gdot = gr / wn1, gwn = -r1 * gdot;   // a reciprocal of a subnormal wn would overflow
+                gW1p += 2.0 * gwn * w1p + gdot * nb1p;
+                gW1n += 2.0 * gwn * w1n + gdot * nb1n;
+                send1p = gdot * w1p; send1n = gdot * w1n;
+            }
+            if (l2) {
+                const double gr = dphi2 * (w2p * gL2p + w2n * gL2n);
+                const double gdot = gr / wn2, gwn = -r2 * gdot;
+                gW2p += 2.0 * gwn * w2p + gdot * nb2p;
+                gW2n += 2.0 * gwn * w2n + gdot * nb2n;
+                send2p = gdot * w2p; send2n = gdot * w2n;
+            }
         }
     }
-    {
+    double gqR_p = 0, gqR_n = 0, gqL_p = 0, gqL_n = 0, grL = 0, gcL = 0, grR = 0, gcR = 0;
+    if (full) {                                   // warp-uniform
         // a wave with s > 0 read its left neighbour, otherwise its right one
         const bool left1 = s1 > 0.0, left2 = s2 > 0.0;
-        const double tl1p = left1 ? send1p : 0.0, tl1n = left1 ? send1n : 0.0;
-        const double tr1p = left1 ? 0.0 : send1p, tr1n = left1 ? 0.0 : send1n;
-        const double tl2p = left2 ? send2p : 0.0, tl2n = left2 ? send2n : 0.0;
-        const double tr2p = left2 ? 0.0 : send2p, tr2n = left2 ? 0.0 : send2n;
-        const double fr1p = __shfl_down_sync(FULL, tl1p, 1), fr1n = __shfl_down_sync(FULL, tl1n, 1);
-        const double fr2p = __shfl_down_sync(FULL, tl2p, 1), fr2n = __shfl_down_sync(FULL, tl2n, 1);
-        const double fl1p = __shfl_up_sync(FULL, tr1p, 1), fl1n = __shfl_up_sync(FULL, tr1n, 1);
-        const double fl2p = __shfl_up_sync(FULL, tr2p, 1), fl2n = __shfl_up_sync(FULL, tr2n, 1);
+        const double fr1p = __shfl_down_sync(FULL, left1 ? send1p : 0.0, 1);
+        const double fr1n = __shfl_down_sync(FULL, left1 ? send1n : 0.0, 1);
+        const double fr2p = __shfl_down_sync(FULL, left2 ? send2p : 0.0, 1);
+        const double fr2n = __shfl_down_sync(FULL, left2 ? send2n : 0.0, 1);
+        const double fl1p = __shfl_up_sync(FULL, left1 ? 0.0 : send1p, 1);
+        const double fl1n = __shfl_up_sync(FULL, left1 ? 0.0 : send1n, 1);
+        const double fl2p = __shfl_up_sync(FULL, left2 ? 0.0 : send2p, 1);
+        const double fl2n = __shfl_up_sync(FULL, left2 ? 0.0 : send2n, 1);
         if (lane < 31) { gW1p += fr1p; gW1n += fr1n; gW2p += fr2p; gW2n += fr2n; }
         if (lane > 0) { gW1p += fl1p; gW1n += fl1n; gW2p += fl2p; gW2n += fl2n; }
-    }
-
-    // ---------------- normal solve, transposed ----------------
-    double gqR_p = 0, gqR_n = 0, gqL_p = 0, gqL_n = 0, grL = 0, gcL = 0, grR = 0, gcR = 0;
-    if (ex) {
-        const double ga1 = -zL * gW1p + gW1n;
-        const double ga2 = zR * gW2p + gW2n;
-        double gzL = -a1 * gW1p, gzR = a2 * gW2p;
-        const double inv = 1.0 / den;
-        const double gd1 = (ga2 - ga1) * inv;
-        const double gd2 = (zR * ga1 + zL * ga2) * inv;
-        gzR += d2 * ga1 * inv;
-        gzL += d2 * ga2 * inv;
-        const double gden = -(a1 * ga1 + a2 * ga2) * inv;
-        gzL += gden;
-        gzR += gden;
-        gqR_p = gd1; gqL_p = -gd1;
-        gqR_n = gd2; gqL_n = -gd2;
-        grL = cL * gzL; gcL = -gs1 + rhoL * gzL;
-        grR = cR * gzR; gcR = gs2 + rhoR * gzR;
+        // ---------------- normal solve, transposed ----------------
+        if (ex) {
+            const double ga1 = -zL * gW1p + gW1n;
+            const double ga2 = zR * gW2p + gW2n;
+            const double inv = 1.0 / den;
+            const double gd1 = (ga2 - ga1) * inv;
+            const double gd2 = (zR * ga1 + zL * ga2) * inv;
+            const double gden = -(a1 * ga1 + a2 * ga2) * inv;
+            const double gzL = -a1 * gW1p + d2 * ga2 * inv + gden;
+            const double gzR = a2 * gW2p + d2 * ga1 * inv + gden;
+            gqR_p = gd1; gqL_p = -gd1;
+            gqR_n = gd2; gqL_n = -gd2;
+            grL = cL * gzL; gcL = -gs1 + rhoL * gzL;
+            grR = cR * gzR; gcR = gs2 + rhoR * gzR;
+        }
     }
 
     // ---------------- gather onto cell k (this lane) from interfaces k and k+1 ----------------
-    const double nq_p = __shfl_down_sync(FULL, gqL_p, 1), nq_n = __shfl_down_sync(FULL, gqL_n, 1);
-    const double nown_r = __shfl_down_sync(FULL, grL + gA_r1, 1), nown_c = __shfl_down_sync(FULL, gcL + gA_c1, 1);
-    const double ndn_r = __shfl_down_sync(FULL, gA_r0, 1), ndn_c = __shfl_down_sync(FULL, gA_c0, 1);
-    const double nup_r = __shfl_down_sync(FULL, gA_r2, 1), nup_c = __shfl_down_sync(FULL, gA_c2, 1);
-    o.dq_p = gqR_p + nq_p;
-    o.dq_n = gqR_n + nq_n;
-    o.ga_own[0] = (grR + gB_r1) + nown_r;
-    o.ga_own[1] = (gcR + gB_c1) + nown_c;
-    o.ga_dn[0] = gB_r0 + ndn_r;
-    o.ga_dn[1] = gB_c0 + ndn_c;
-    o.ga_up[0] = gB_r2 + nup_r;
-    o.ga_up[1] = gB_c2 + nup_c;
+    o.dq_p = gqR_p + __shfl_down_sync(FULL, gqL_p, 1);
+    o.dq_n = gqR_n + __shfl_down_sync(FULL, gqL_n, 1);
+    o.ga_own[0] = (grR + gB_r1) + __shfl_down_sync(FULL, grL + gA_r1, 1);
+    o.ga_own[1] = (gcR + gB_c1) + __shfl_down_sync(FULL, gcL + gA_c1, 1);
+    o.ga_dn[0] = gB_r0 + __shfl_down_sync(FULL, gA_r0, 1);
+    o.ga_dn[1] = gB_c0 + __shfl_down_sync(FULL, gA_c0, 1);
+    o.ga_up[0] = gB_r2 + __shfl_down_sync(FULL, gA_r2, 1);
+    o.ga_up[1] = gB_c2 + __shfl_down_sync(FULL, gA_c2, 1);
+}
+
+// One sweep direction of a tile: lines first..last in chunks of 8 (one per
+// warp).  Each chunk stages its lines' aux gradients for the neighbouring
+// lines (up, dn) in one half of XS, passes one barrier, and then every line
+// adds to its own row: its own terms, up from the line below and dn from the
+// line above; the chunk's first line also adds its dn to the row below the
+// chunk and its last line its up to the row above (those rows belong to the
+// neighbouring chunks, whose writes the barriers order).
+template <int IXY>
+__device__ __forceinline__ void adj_sweep(const AdjArgs& a, const double* __restrict__ q,
+                                          const double* __restrict__ lin, int i0, int j0, int ilo, int ihi, int jlo,
+                                          int jhi, double* GQ, double* GA, double* XS, int& chunk)
+{
+    constexpr int MN = IXY == 1 ? 1 : 2;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int o0 = IXY == 1 ? j0 : i0;                 // lines run across the tile
+    const int olen = IXY == 1 ? a.my : a.mx;
+    const int llo = IXY == 1 ? jlo : ilo, lhi = IXY == 1 ? jhi : ihi;    // own lines
+    const int clo = IXY == 1 ? ilo : jlo, chi = IXY == 1 ? ihi : jhi;    // own cells along a line
+    const int first = o0 - 1 > -1 ? o0 - 1 : -1;
+    const int last = o0 + AT < olen ? o0 + AT : olen;
+    auto sidx = [&](int c, int l) {
+        return IXY == 1 ? (l - j0 + 2) * AR + (c - i0 + 2) : (c - j0 + 2) * AR + (l - i0 + 2);
+    };
+    for (int c0 = first; c0 <= last; c0 += ANT / 32, chunk++) {
+        const int line = c0 + warp;
+        const int clast = c0 + ANT / 32 - 1 < last ? c0 + ANT / 32 - 1 : last;
+        const bool ok = line <= last;
+        const bool own = ok && line >= llo && line < lhi;
+        LineOut o;
+        adj_line<IXY>(a, q, lin, i0, j0, line, ok, own, o);
+        const int c = (IXY == 1 ? i0 : j0) - 2 + lane;
+        const bool cown = ok && c >= clo && c < chi;
+        double* X = XS + (chunk & 1) * 4 * ANT;
+        X[0 * ANT + tid] = o.ga_up[0];
+        X[1 * ANT + tid] = o.ga_up[1];
+        X[2 * ANT + tid] = o.ga_dn[0];
+        X[3 * ANT + tid] = o.ga_dn[1];
+        if (cown && own) {
+            const int s = sidx(c, line);
+            GQ[s] += o.dq_p;
+            GQ[MN * AR * AR + s] += o.dq_n;
+        }
+        __syncthreads();
+        if (cown) {
+            if (own) {
+                double g0 = o.ga_own[0], g1 = o.ga_own[1];
+                if (line > c0) { g0 += X[0 * ANT + tid - 32]; g1 += X[1 * ANT + tid - 32]; }
+                if (line < clast) { g0 += X[2 * ANT + tid + 32]; g1 += X[3 * ANT + tid + 32]; }
+                const int s = sidx(c, line);
+                GA[s] += g0;
+                GA[AR * AR + s] += g1;
+            }
+            if (line == c0 && line - 1 >= llo && line - 1 < lhi) {
+                const int s = sidx(c, line - 1);
+                GA[s] += o.ga_dn[0];
+                GA[AR * AR + s] += o.ga_dn[1];
+            }
+            if (line == clast && line + 1 >= llo && line + 1 < lhi) {
+                const int s = sidx(c, line + 1);
+                GA[s] += o.ga_up[0];
+                GA[AR * AR + s] += o.ga_up[1];
+            }
+        }
+    }
 }
 
 __global__ void __launch_bounds__(ANT, CLAW2_ADJ_MINB) adjoint_kernel(AdjArgs a)
 {
-    __shared__ double GQ[3 * AR * AR];
-    __shared__ double GA[2 * AR * AR];
+    extern __shared__ double adj_smem[];
+    double* GQ = adj_smem;                    // 3 x AR x AR state adjoint
+    double* GA = GQ + 3 * AR * AR;            // 2 x AR x AR aux gradient
+    double* XS = GA + 2 * AR * AR;            // 2 x 4 x ANT cross-line exchange
     const int shot = blockIdx.z;
     const double* __restrict__ q = a.q + shot * a.qstride;
     const double* __restrict__ lin = a.lam_in + shot * a.qstride;
     double* lout = a.lam_out + shot * a.qstride;
     double* gaux = a.gaux + shot * a.gstride;
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int tid = threadIdx.x;
     const int i0 = blockIdx.x * AT, j0 = blockIdx.y * AT;
     // cells this CTA owns: its tile, plus the ghost ring on domain sides
     const int ilo = i0 == 0 ? -2 : i0, ihi = i0 + AT >= a.mx ? a.mx + 2 : i0 + AT;
     const int jlo = j0 == 0 ? -2 : j0, jhi = j0 + AT >= a.my ? a.my + 2 : j0 + AT;
     const long long P = a.plane;
-    auto sidx = [&](int i, int j) { return (j - j0 + 2) * AR + (i - i0 + 2); };
 
     for (int t = tid; t < AR * AR; t += ANT) {
         const int i = i0 - 2 + t % AR, j = j0 - 2 + t / AR;
@@ -355,73 +426,10 @@ __global__ void __launch_bounds__(ANT, CLAW2_ADJ_MINB) adjoint_kernel(AdjArgs a)
         GA[AR * AR + t] = 0.0;
     }
     __syncthreads();
-
-    // ---- x-slices: rows j0-1 .. j0+AT (the forward has rows -1 .. my)
-    {
-        const int first = j0 - 1 > -1 ? j0 - 1 : -1;
-        const int last = j0 + AT < a.my ? j0 + AT : a.my;
-        for (int c0 = first; c0 <= last; c0 += ANT / 32) {
-            const int line = c0 + warp;
-            const bool ok = line <= last;
-            LineOut o;
-            adj_line<1>(a, q, lin, i0, j0, line, ok, o);
-            const int c = i0 - 2 + lane;
-            const bool cown = ok && c >= ilo && c < ihi;
-            if (cown && line >= jlo && line < jhi) {
-                const int s = sidx(c, line);
-                GQ[s] += o.dq_p;
-                GQ[AR * AR + s] += o.dq_n;
-                GA[s] += o.ga_own[0];
-                GA[AR * AR + s] += o.ga_own[1];
-            }
-            __syncthreads();
-            if (cown && line + 1 >= jlo && line + 1 < jhi) {
-                const int s = sidx(c, line + 1);
-                GA[s] += o.ga_up[0];
-                GA[AR * AR + s] += o.ga_up[1];
-            }
-            __syncthreads();
-            if (cown && line - 1 >= jlo && line - 1 < jhi) {
-                const int s = sidx(c, line - 1);
-                GA[s] += o.ga_dn[0];
-                GA[AR * AR + s] += o.ga_dn[1];
-            }
-            __syncthreads();
-        }
-    }
-    // ---- y-slices: columns i0-1 .. i0+AT
-    {
-        const int first = i0 - 1 > -1 ? i0 - 1 : -1;
-        const int last = i0 + AT < a.mx ? i0 + AT : a.mx;
-        for (int c0 = first; c0 <= last; c0 += ANT / 32) {
-            const int line = c0 + warp;
-            const bool ok = line <= last;
-            LineOut o;
-            adj_line<2>(a, q, lin, i0, j0, line, ok, o);
-            const int c = j0 - 2 + lane;
-            const bool cown = ok && c >= jlo && c < jhi;
-            if (cown && line >= ilo && line < ihi) {
-                const int s = sidx(line, c);
-                GQ[s] += o.dq_p;
-                GQ[2 * AR * AR + s] += o.dq_n;
-                GA[s] += o.ga_own[0];
-                GA[AR * AR + s] += o.ga_own[1];
-            }
-            __syncthreads();
-            if (cown && line + 1 >= ilo && line + 1 < ihi) {
-                const int s = sidx(line + 1, c);
-                GA[s] += o.ga_up[0];
-                GA[AR * AR + s] += o.ga_up[1];
-            }
-            __syncthreads();
-            if (cown && line - 1 >= ilo && line - 1 < ihi) {
-                const int s = sidx(line - 1, c);
-                GA[s] += o.ga_dn[0];
-                GA[AR * AR + s] += o.ga_dn[1];
-            }
-            __syncthreads();
-        }
-    }
+    int chunk = 0;
+    adj_sweep<1>(a, q, lin, i0, j0, ilo, ihi, jlo, jhi, GQ, GA, XS, chunk);     // x-slices: rows
+    adj_sweep<2>(a, q, lin, i0, j0, ilo, ihi, jlo, jhi, GQ, GA, XS, chunk);     // y-slices: columns
+    __syncthreads();
 
     for (int t = tid; t < AR * AR; t += ANT) {
         const int i = i0 - 2 + t % AR, j = j0 - 2 + t / AR;
@@ -679,8 +687,15 @@ int claw2_shots_adjoint_step(const claw2_problem* p, int nshots, long long shot_
     a.dtdx = dt / p->dx; a.dtdy = dt / p->dy;
     a.order = p->order; a.trans = p->transverse;
     a.mthlim[0] = p->mthlim[0]; a.mthlim[1] = p->mthlim[1];
+    constexpr int smem = (5 * AR * AR + 2 * 4 * ANT) * 8;
+    static bool configured = false;
+    if (!configured) {
+        if (cudaFuncSetAttribute(adjoint_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
+            return CLAW2_ERR_CUDA;
+        configured = true;
+    }
     const dim3 grid((p->mx + AT - 1) / AT, (p->my + AT - 1) / AT, nshots);
-    adjoint_kernel<<<grid, ANT, 0, Sx(stream)>>>(a);
+    adjoint_kernel<<<grid, ANT, smem, Sx(stream)>>>(a);
     return cudaGetLastError() == cudaSuccess ? CLAW2_OK : CLAW2_ERR_CUDA;
 }
 
