@@ -202,6 +202,39 @@ CLAW2_EXPORT int claw2_advance(const claw2_problem* p, double* q0, double* q1,
                   const double* aux, claw2_control* ctrl, void* scratch,
                   int nsteps, void* stream);
 
+/* Device-side forms of two application callbacks of the reference's Euler
+ * shock-bubble app, so that a run using them needs no host round trip per step
+ * (the reference passes Python functions: solver.step_source and a custom
+ * boundary callback, apps/euler_2d/shockbubble.py:68-124).
+ *  - source CLAW2_SRC_EULER_RADIAL: the geometric source of the Euler equations
+ *    with radial symmetry, integrated with the app's two-stage second-order
+ *    Runge-Kutta step (step_Euler_radial, shockbubble.py:89-124) on every
+ *    interior cell after the hyperbolic step (Godunov splitting, source_split
+ *    = 1), the radial coordinate read from aux component source_aux.  It is
+ *    fused into the step's final write; a rejected step's output is discarded
+ *    whole.  (One difference: the reference skips the source of a step whose
+ *    CFL number equals cfl_max exactly and still accepts the step.)
+ *  - a fixed inflow state on a side is expressed as a custom side (bc 0)
+ *    whose ghost cells the caller fills once, in both state buffers: the step
+ *    never writes the ghost cells of custom sides. */
+enum claw2_source {
+    CLAW2_SRC_NONE = 0,
+    CLAW2_SRC_EULER_RADIAL = 1
+};
+
+typedef struct claw2_hooks {
+    int32_t source;        /* claw2_source                                  */
+    int32_t source_aux;    /* aux component holding the radial coordinate   */
+    int32_t reserved_[2];
+} claw2_hooks;
+
+/* claw2_advance with the source term of `hooks` applied to each step.
+ * CLAW2_ERR_UNSUPPORTED for a source the Riemann solver cannot take
+ * (CLAW2_SRC_EULER_RADIAL needs the Euler solvers and aux). */
+CLAW2_EXPORT int claw2_advance_hooked(const claw2_problem* p, double* q0, double* q1, const double* aux,
+                                      claw2_control* ctrl, void* scratch, int nsteps, const claw2_hooks* hooks,
+                                      void* stream);
+
 /* Host-side initialisation of a controller for evolve_to_time(solution, tend)
  * (solver.py:600-641): status reset, fixed-dt step count, first clamp. */
 CLAW2_EXPORT int claw2_control_init(claw2_control* c, double t, double dt, double tend,

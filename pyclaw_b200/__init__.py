@@ -9,7 +9,7 @@ The public names mirror ``clawpack.pyclaw`` (src/pyclaw/__init__.py):
 The step itself runs as hand-written CUDA kernels from libclaw2.so (built by
 ``python -m pyclaw_b200.build``); there is no CPU fallback.
 """
-from . import limiters, riemann  # noqa: F401
+from . import hooks, limiters, riemann  # noqa: F401
 from .cfl import CFL  # noqa: F401
 from .classic import ClawSolver, ClawSolver2D  # noqa: F401
 from .controller import Controller  # noqa: F401

@@ -63,6 +63,20 @@ class Problem(ctypes.Structure):
     ]
 
 
+# source terms of claw2_hooks (enum claw2_source)
+SRC_NONE = 0
+SRC_EULER_RADIAL = 1
+
+
+class Hooks(ctypes.Structure):
+    """struct claw2_hooks."""
+    _fields_ = [
+        ("source", ctypes.c_int32),
+        ("source_aux", ctypes.c_int32),
+        ("reserved_", ctypes.c_int32 * 2),
+    ]
+
+
 class Layout(ctypes.Structure):
     """struct claw2_layout."""
     _fields_ = [

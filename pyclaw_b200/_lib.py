@@ -32,6 +32,8 @@ PROTOTYPES = [
     ("claw2_step", ctypes.c_int, [_P, _dp, _dp, _dp, _dbl, _vp, _dp, _vp]),
     ("claw2_step_noalloc", ctypes.c_int, [_P, _dp, _dp, _dp, _dbl, _dp, _vp]),
     ("claw2_advance", ctypes.c_int, [_P, _dp, _dp, _dp, _vp, _vp, ctypes.c_int, _vp]),
+    ("claw2_advance_hooked", ctypes.c_int, [_P, _dp, _dp, _dp, _vp, _vp, ctypes.c_int, ctypes.POINTER(_abi.Hooks),
+                                            _vp]),
     ("claw2_control_init", ctypes.c_int, [_C, _dbl, _dbl, _dbl, _dbl, _dbl, _dbl, ctypes.c_int,
                                           ctypes.c_int, _i64, _dbl]),
     ("claw2_ref_to_device", ctypes.c_int, [_P, ctypes.c_int, _dp, _dp, _vp]),

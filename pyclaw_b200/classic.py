@@ -5,7 +5,8 @@ ClawSolver2D keeps the reference's attributes and call contract
 stays in GPU memory and the step is the fused sm_100a kernel of libclaw2.so.
 evolve_to_time runs the whole step-size control loop on the device (one kernel
 launch per step, no host round trip) unless a Python callback (before_step,
-step_source, a custom boundary condition, gauges) has to run between steps.
+step_source, a custom boundary condition, gauges) has to run between steps;
+the callbacks of pyclaw_b200.hooks run on the device.
 """
 import ctypes
 import warnings
@@ -213,8 +214,24 @@ class ClawSolver2D(ClawSolver):
             raise FloatingPointError("the step produced a non-finite state")
 
     # ---- device-controlled loop ---------------------------------------------
+    def _device_hooks(self):
+        """The claw2_hooks that let the device run this solver's callbacks
+        itself (hooks.EulerRadialSource, hooks.FixedStateBC), or None when
+        some callback has to run on the host."""
+        from .hooks import EulerRadialSource, FixedStateBC
+        h = _abi.Hooks()
+        if self.step_source is not None:
+            if not isinstance(self.step_source, EulerRadialSource) or self.source_split != 1:
+                return None
+            h.source = self.step_source.kind
+            h.source_aux = self.step_source.radius_aux
+        for bcs, fns in ((self.bc_lower, self.user_bc_lower), (self.bc_upper, self.user_bc_upper)):
+            if BC.custom in list(bcs) and not isinstance(fns, FixedStateBC):
+                return None
+        return h
+
     def _device_loop_ok(self, solution):
-        return (self.before_step is None and self.step_source is None and not self._custom_bcs()
+        return (self.before_step is None and self._device_hooks() is not None
                 and len(solution.state.grid.gauges) == 0)
 
     def evolve_to_time(self, solution, tend=None):
@@ -237,7 +254,19 @@ class ClawSolver2D(ClawSolver):
             raise Exception('Variable time-stepping and desired CFL > maximum CFL')
         if not self.dt_variable:
             self.max_steps = int(c.max_steps)
-        out = self._dev.evolve(c)
+        hooks = None
+        if self.step_source is not None or self._custom_bcs():
+            hooks = self._device_hooks()
+            if self._custom_bcs():
+                # fixed-state sides: set once in both state buffers; the
+                # step never writes the ghost cells of custom sides
+                dev = self._dev
+                qbc = dev.ghosted_ref()
+                self._fill_host_bcs(state, qbc, self.bc_lower, self.bc_upper, self.user_bc_lower,
+                                    self.user_bc_upper, negate=True)
+                dev.set_ghosted_ref(qbc, dev.cur)
+                dev.set_ghosted_ref(qbc, 1 - dev.cur)
+        out = self._dev.evolve(c, hooks=hooks)
         solution.t = out.t
         self.dt = out.dt
         self.cfl.update_global_max(out.cfl)

@@ -464,6 +464,33 @@ int claw2_advance(const claw2_problem* p, double* q0, double* q1, const double* 
     return CLAW2_OK;
 }
 
+int claw2_advance_hooked(const claw2_problem* p, double* q0, double* q1, const double* aux, claw2_control* ctrl,
+                         void* scratch, int nsteps, const claw2_hooks* hooks, void* stream)
+{
+    int rc = claw2_validate(p);
+    if (rc) return rc;
+    if (!q0 || !q1 || !ctrl || !scratch || !hooks || (p->num_aux > 0 && !aux) || nsteps < 0) return CLAW2_ERR_INVALID;
+    if (hooks->source != CLAW2_SRC_NONE && hooks->source != CLAW2_SRC_EULER_RADIAL) return CLAW2_ERR_INVALID;
+    if (hooks->source == CLAW2_SRC_EULER_RADIAL &&
+        ((p->rp != CLAW2_RP_EULER_4WAVE && p->rp != CLAW2_RP_EULER_5WAVE) || hooks->source_aux < 0 ||
+         hooks->source_aux >= p->num_aux))
+        return CLAW2_ERR_UNSUPPORTED;
+    StepArgs a;
+    fill_args(p, q0, a);
+    a.q0 = q0; a.q1 = q1; a.aux = aux; a.ctrl = ctrl;
+    a.ticket = static_cast<unsigned int*>(scratch);
+    a.partials = reinterpret_cast<double*>(static_cast<char*>(scratch) + 64);
+    a.src = hooks->source;
+    a.src_aux = hooks->source_aux;
+    for (int n = 0; n < nsteps; n++) {
+        if ((rc = launch_step(p, a, S(stream)))) return rc;
+        if (!a.ghost_fused &&
+            (rc = launch_fill(p, nullptr, p->num_eqn, p->bc_lower, p->bc_upper, false, q0, q1, ctrl, S(stream))))
+            return rc;
+    }
+    return CLAW2_OK;
+}
+
 int claw2_control_init(claw2_control* c, double t, double dt, double tend, double cfl_max, double cfl_desired,
                        double dt_max, int dt_variable, int take_one_step, int64_t max_steps, double prev_cfl)
 {

@@ -54,6 +54,7 @@ struct StepArgs {
     double prm[CLAW2_MAX_PARAMS];
     int ghost_fused;
     int bcl[2], bcu[2];
+    int src, src_aux;      // source term fused into the final write (claw2_source)
 };
 
 template <int IXY> struct Phase;
@@ -519,9 +520,39 @@ struct TileId {
 // row 0 = tile row j0) and their ghost images, then the block CFL max and the
 // last-arriving CTA's reduction over all CTAs (and, in controlled mode, the
 // device-side time-step controller).
+// Geometric source of the Euler equations with radial symmetry (2D, so the
+// factor ndim-1 is 1), two-stage second-order Runge-Kutta step of the
+// reference app (apps/euler_2d/shockbubble.py:89-124), with its operation
+// order; rad = the cell's radial coordinate.
+template <int MEQN>
+CLAW2_HD void euler_radial_source(double (&v)[MEQN], double rad, double gamma1, double dt)
+{
+    if constexpr (MEQN >= 4) {
+        const double dt2 = dt / 2.0;
+        double rho = v[0];
+        double u = v[1] / rho;
+        double w = v[2] / rho;
+        double press = gamma1 * (v[3] - 0.5 * rho * (u * u + w * w));
+        const double h = dt2 * 1.0 / rad;
+        const double s0 = v[0] - h * v[2];
+        const double s1 = v[1] - h * rho * u * w;
+        const double s2 = v[2] - h * rho * w * w;
+        const double s3 = v[3] - h * w * (v[3] + press);
+        rho = s0;
+        u = s1 / rho;
+        w = s2 / rho;
+        press = gamma1 * (s3 - 0.5 * rho * (u * u + w * w));
+        const double f = dt * 1.0 / rad;
+        v[0] = v[0] - f * s2;
+        v[1] = v[1] - f * rho * u * w;
+        v[2] = v[2] - f * rho * w * w;
+        v[3] = v[3] - f * w * (s3 + press);
+    }
+}
+
 template <int MEQN, int TX, int TY, int NT, class Ctx>
 CLAW2_HD void finish_tile(const StepArgs& a, Ctx& ctx, const TileId& tile, const double* Qx, int QSTR, double* red,
-                          double* qout, int i0, int j0, double cflm)
+                          double* qout, int i0, int j0, double cflm, double dt)
 {
     const int tid = ctx.tid();
     int bad = 0;
@@ -531,10 +562,12 @@ CLAW2_HD void finish_tile(const StepArgs& a, Ctx& ctx, const TileId& tile, const
         if (i >= a.mx || j >= a.my) continue;
         double v[MEQN];
 #pragma unroll
-        for (int m = 0; m < MEQN; m++) {
-            v[m] = Qx[m * QSTR + cj * TX + ci];
+        for (int m = 0; m < MEQN; m++) v[m] = Qx[m * QSTR + cj * TX + ci];
+        if (a.src == CLAW2_SRC_EULER_RADIAL)
+            euler_radial_source<MEQN>(v, a.aux[qoff(a, a.src_aux, i, j)], a.prm[1], dt);
+#pragma unroll
+        for (int m = 0; m < MEQN; m++)
             if (!isfinite(v[m])) bad = 1;
-        }
         write_cell<MEQN>(a, qout, i, j, v);
     }
 
@@ -648,7 +681,7 @@ CLAW2_HD void step_tile_at(const StepArgs& a, Ctx& ctx, const TileId& tile)
         }
     }
 
-    finish_tile<MEQN, TX, TY, NT>(a, ctx, tile, Qx + (-QROW0) * TX, QROWS * TX, red, qout, i0, j0, cflm);
+    finish_tile<MEQN, TX, TY, NT>(a, ctx, tile, Qx + (-QROW0) * TX, QROWS * TX, red, qout, i0, j0, cflm, dt);
 }
 
 template <class RP, int TX, int TY, int NT, bool SPLIT, class Ctx>

@@ -338,7 +338,7 @@ CLAW2_HD void light_tile_at(const StepArgs& a, Ctx& ctx, const TileId& tile)
         }
     }
     ctx.sync();
-    finish_tile<3, TX, TY, NT>(a, ctx, tile, Qx, TX * TY, red, qout, i0, j0, cflm);
+    finish_tile<3, TX, TY, NT>(a, ctx, tile, Qx, TX * TY, red, qout, i0, j0, cflm, dt);
 }
 
 }  // namespace claw2

@@ -135,8 +135,9 @@ class DeviceState(object):
         cfl = float(self.cfl_dev.item())
         return cfl, nxt
 
-    def evolve(self, control, max_batch=64):
-        """Run the device-controlled loop until control is done; returns the final Control."""
+    def evolve(self, control, max_batch=64, hooks=None):
+        """Run the device-controlled loop until control is done; returns the
+        final Control.  hooks: a claw2_hooks (source term run on the device)."""
         torch = _torch()
         control.cur = self.cur
         host = _abi.Control.from_address(self.ctrl_host.data_ptr())
@@ -145,9 +146,15 @@ class DeviceState(object):
         stream = torch.cuda.current_stream(self.device)
         batch = 8
         while True:
-            _lib.check(self.lib.claw2_advance(ctypes.byref(self.p), self.ptr(self.q[0]), self.ptr(self.q[1]),
-                                              self.ptr(self.aux), self.ptr(self.ctrl), self.ptr(self.scratch),
-                                              int(batch), self.stream), "claw2_advance")
+            if hooks is None:
+                _lib.check(self.lib.claw2_advance(ctypes.byref(self.p), self.ptr(self.q[0]), self.ptr(self.q[1]),
+                                                  self.ptr(self.aux), self.ptr(self.ctrl), self.ptr(self.scratch),
+                                                  int(batch), self.stream), "claw2_advance")
+            else:
+                _lib.check(self.lib.claw2_advance_hooked(ctypes.byref(self.p), self.ptr(self.q[0]),
+                                                         self.ptr(self.q[1]), self.ptr(self.aux), self.ptr(self.ctrl),
+                                                         self.ptr(self.scratch), int(batch), ctypes.byref(hooks),
+                                                         self.stream), "claw2_advance_hooked")
             self.ctrl_host.copy_(self.ctrl, non_blocking=True)
             stream.synchronize()
             if host.done:

@@ -14,7 +14,7 @@ GOLD = os.path.join(os.path.dirname(__file__), "golden")
 
 
 def _api_run(p, q, aux, run, tfinal, nout, split, trans=2, rp=None, bcs=None, src=None, keep=True,
-             bounds=((0.0, 1.0), (0.0, 1.0))):
+             bounds=((0.0, 1.0), (0.0, 1.0)), before_step=None):
     """Build the same problem through the public API and run it on the GPU."""
     x = pc.Dimension('x', bounds[0][0], bounds[0][1], p.mx)
     y = pc.Dimension('y', bounds[1][0], bounds[1][1], p.my)
@@ -42,6 +42,8 @@ def _api_run(p, q, aux, run, tfinal, nout, split, trans=2, rp=None, bcs=None, sr
         solver.user_bc_lower = bcs
     if src:
         solver.step_source = src
+    if before_step is not None:
+        solver.before_step = before_step
     claw = pc.Controller()
     claw.solution = pc.Solution(state, domain)
     claw.solver = solver
@@ -101,6 +103,44 @@ def test_shockbubble_app_custom_bc_and_source(orc):
     assert np.array_equal(got, frames[1])
     gold = np.load(os.path.join(GOLD, "shockbubble_density.npz"))["density"]
     assert K.check_diff(0, np.linalg.norm(gold - got[0]), abstol=1e-12) is None
+
+
+def _shockbubble_hooks():
+    rinf, vinf, einf = K._shock_state()
+    inflow = pc.hooks.FixedStateBC([rinf, rinf * vinf, 0., einf, 0.], side="lower")
+    return inflow, pc.hooks.EulerRadialSource(radius_aux=0)
+
+
+def test_shockbubble_app_on_the_device(orc):
+    """The same app with its inflow condition and radial source given as the
+    device-side hooks: the whole evolve_to_time loop stays on the GPU (source
+    fused into the step kernel) and the result equals the oracle's run with
+    the app's own Python callbacks, and the reference's file to 1e-12."""
+    p, q, aux, run, bcs, src = K.shockbubble_setup()
+    inflow, source = _shockbubble_hooks()
+    claw, solver = _api_run(p, q, aux, run, 0.2, 1, split=True, rp=pc.riemann.rp2_euler_5wave,
+                            bcs=inflow, src=source, bounds=((0.0, 2.0), (0.0, 0.5)))
+    assert solver._device_loop_ok(claw.solution)
+    got = claw.frames[1].state.q
+    ref = orc.Run(p, q, aux, bc_callbacks=bcs, step_source=src, **run)
+    frames = ref.run(0.2, num_output_times=1)
+    assert np.array_equal(got, frames[1]), np.max(np.abs(got - frames[1]))
+    assert solver.status['numsteps'] == ref.steps_taken
+    gold = np.load(os.path.join(GOLD, "shockbubble_density.npz"))["density"]
+    assert K.check_diff(0, np.linalg.norm(gold - got[0]), abstol=1e-12) is None
+
+
+def test_shockbubble_hooks_on_the_host_path(orc):
+    """The hook objects are ordinary callbacks too: with a before_step
+    callback forcing the host-driven loop the result is the same."""
+    p, q, aux, run, bcs, src = K.shockbubble_setup()
+    inflow, source = _shockbubble_hooks()
+    claw, solver = _api_run(p, q, aux, run, 0.2, 1, split=True, rp=pc.riemann.rp2_euler_5wave,
+                            bcs=inflow, src=source, bounds=((0.0, 2.0), (0.0, 0.5)), before_step=lambda s, st: None)
+    assert not solver._device_loop_ok(claw.solution)
+    ref = orc.Run(p, q, aux, bc_callbacks=bcs, step_source=src, **run)
+    frames = ref.run(0.2, num_output_times=1)
+    assert np.array_equal(claw.frames[1].state.q, frames[1])
 
 
 def test_config1_acoustics_full_run_parity(orc):
