@@ -142,10 +142,16 @@ __device__ __forceinline__ double split_T(double asdq, double bm_p, double bm_t,
 // One slice line of the adjoint.  full = false for a line whose cells the
 // tile does not own: only its transverse splits' aux gradients on the
 // neighbouring lines (ga_dn, ga_up) are needed.
+// y lines read their inputs from a staged copy (adj_stage_y): field f, row r
+// (the lane's left cell k-1 at r = lane), column c (the line at c = sc)
+constexpr int YR = 33;                 // rows j0-3 .. j0+AT+2
+constexpr int YP = ANT / 32 + 3;       // columns c0-1 .. c0+8, padded to an odd pitch
+constexpr int YF = 7;                  // p, v, rho, c, lambda_p, lambda_u, lambda_v
+
 template <int IXY>
 __device__ __forceinline__ void adj_line(const AdjArgs& a, const double* __restrict__ q,
-                                         const double* __restrict__ lin, int i0, int j0, int line, bool lineok,
-                                         bool full, LineOut& o)
+                                         const double* __restrict__ lin, const double* __restrict__ STG, int sc,
+                                         int i0, int j0, int line, bool lineok, bool full, LineOut& o)
 {
     constexpr int MN = IXY == 1 ? 1 : 2;     // normal velocity component
     constexpr int MT = IXY == 1 ? 2 : 1;     // transverse velocity component
@@ -163,16 +169,29 @@ __device__ __forceinline__ void adj_line(const AdjArgs& a, const double* __restr
     const bool trans = a.trans > 0;
     const long long oR = IXY == 1 ? cell(a, k, line) : cell(a, line, k);
     const long long oL = oR - along;
+    // side 0: cell k-1, side 1: cell k; dl: the line below (-1), on (0), above (+1)
+    auto Gq = [&](int m, int side) -> double {          // m 0: pressure, 1: normal velocity
+        if constexpr (IXY == 2) return STG[(m * YR + lane + side) * YP + sc];
+        else return q[(side ? oR : oL) + (m ? MN * P : 0)];
+    };
+    auto Ga = [&](int f, int side, int dl) -> double {  // f 0: rho, 1: c
+        if constexpr (IXY == 2) return STG[((2 + f) * YR + lane + side) * YP + sc + dl];
+        else return aux[(side ? oR : oL) + dl * across + f * P];
+    };
+    auto Gl = [&](int m, int side, int dl) -> double {  // m 0: pressure, 1: transverse, 2: normal
+        if constexpr (IXY == 2) return STG[((4 + m) * YR + lane + side) * YP + sc + dl];
+        else return lin[(side ? oR : oL) + dl * across + (m == 0 ? 0 : (m == 1 ? MT : MN)) * P];
+    };
 
     // ---------------- forward recompute: normal solve (RpVcAcoustics::rpn2) ----------------
     double rhoL = 0.0, cL = 0.0, rhoR = 0.0, cR = 0.0, zL = 0.0, zR = 0.0, d2 = 0.0, den = 1.0, a1 = 0.0, a2 = 0.0;
     if (ex) {
-        rhoL = aux[oL]; cL = aux[oL + P];
-        rhoR = aux[oR]; cR = aux[oR + P];
+        rhoL = Ga(0, 0, 0); cL = Ga(1, 0, 0);
+        rhoR = Ga(0, 1, 0); cR = Ga(1, 1, 0);
         zR = rhoR * cR;
         zL = rhoL * cL;
-        const double d1 = q[oR] - q[oL];
-        d2 = q[oR + MN * P] - q[oL + MN * P];
+        const double d1 = Gq(0, 1) - Gq(0, 0);
+        d2 = Gq(1, 1) - Gq(1, 0);
         den = zL + zR;
         a1 = (-d1 + zR * d2) / den;
         a2 = (d1 + zL * d2) / den;
@@ -222,8 +241,8 @@ __device__ __forceinline__ void adj_line(const AdjArgs& a, const double* __restr
     // reciprocals of cell k (cell k-1's come from the lane to the left)
     double rB0 = 0.0, cB0 = 0.0, rB2 = 0.0, cB2 = 0.0, iB1 = 0.0, iB2 = 0.0;
     if (ex && trans) {
-        rB0 = aux[oR - across]; cB0 = aux[oR - across + P];
-        rB2 = aux[oR + across]; cB2 = aux[oR + across + P];
+        rB0 = Ga(0, 1, -1); cB0 = Ga(1, 1, -1);
+        rB2 = Ga(0, 1, 1); cB2 = Ga(1, 1, 1);
         iB1 = 1.0 / (rB0 * cB0 + zR);
         iB2 = 1.0 / (zR + rB2 * cB2);
     }
@@ -233,16 +252,16 @@ __device__ __forceinline__ void adj_line(const AdjArgs& a, const double* __restr
     double gApd = 0.0, gPpd = 0.0;                                // d/d asdq(1) of A and P
     if (ex && trans) {
         const double h = 0.5 * dtn;
-        const double LAp0 = lin[oL - across], LAt0 = lin[oL - across + MT * P];
-        const double LAp1 = lin[oL], LAt1 = lin[oL + MT * P];
-        const double LAp2 = lin[oL + across], LAt2 = lin[oL + across + MT * P];
-        const double LBp0 = lin[oR - across], LBt0 = lin[oR - across + MT * P];
-        const double LBp1 = lin[oR], LBt1 = lin[oR + MT * P];
-        const double LBp2 = lin[oR + across], LBt2 = lin[oR + across + MT * P];
+        const double LAp0 = Gl(0, 0, -1), LAt0 = Gl(1, 0, -1);
+        const double LAp1 = Gl(0, 0, 0), LAt1 = Gl(1, 0, 0);
+        const double LAp2 = Gl(0, 0, 1), LAt2 = Gl(1, 0, 1);
+        const double LBp0 = Gl(0, 1, -1), LBt0 = Gl(1, 1, -1);
+        const double LBp1 = Gl(0, 1, 0), LBt1 = Gl(1, 1, 0);
+        const double LBp2 = Gl(0, 1, 1), LBt2 = Gl(1, 1, 1);
         const double Ap = s1 * w1p + (cor ? cqp : 0.0);
         const double Pp = s2 * w2p - (cor ? cqp : 0.0);
-        const double rA0 = aux[oL - across], cA0 = aux[oL - across + P];
-        const double rA2 = aux[oL + across], cA2 = aux[oL + across + P];
+        const double rA0 = Ga(0, 0, -1), cA0 = Ga(1, 0, -1);
+        const double rA2 = Ga(0, 0, 1), cA2 = Ga(1, 0, 1);
         // g1(c) = dtt (lam(c) - lam(c, below)), g2(c) = dtt (lam(c, above) - lam(c)); d/d bm = -h g1, d/d bp = -h g2
         gApd = split_T(Ap, -h * (dtt * (LAp1 - LAp0)), -h * (dtt * (LAt1 - LAt0)), -h * (dtt * (LAp2 - LAp1)),
                        -h * (dtt * (LAt2 - LAt1)), rA0, cA0, rhoL, cL, rA2, cA2, iA1, iA2, gA_r0, gA_c0, gA_r1, gA_c1,
@@ -256,8 +275,8 @@ __device__ __forceinline__ void adj_line(const AdjArgs& a, const double* __restr
     double gW1p = 0, gW1n = 0, gW2p = 0, gW2n = 0, gs1 = 0, gs2 = 0;
     double send1p = 0.0, send1n = 0.0, send2p = 0.0, send2n = 0.0;   // to the upwind neighbour's wave
     if (full && ex) {
-        const double LAp1 = lin[oL], LAn1 = lin[oL + MN * P];
-        const double LBp1 = lin[oR], LBn1 = lin[oR + MN * P];
+        const double LAp1 = Gl(0, 0, 0), LAn1 = Gl(2, 0, 0);
+        const double LBp1 = Gl(0, 1, 0), LBn1 = Gl(2, 1, 0);
         const double gAm_p = -dtn * LAp1 + gApd, gAm_n = -dtn * LAn1;   // d/d amdq
         const double gAp_p = -dtn * LBp1 + gPpd, gAp_n = -dtn * LBn1;   // d/d apdq
         gW1p = s1 * gAm_p; gW1n = s1 * gAm_n; gW2p = s2 * gAp_p; gW2n = s2 * gAp_n;
@@ -332,6 +351,38 @@ __device__ __forceinline__ void adj_line(const AdjArgs& a, const double* __restr
     o.ga_up[1] = gB_c2 + __shfl_down_sync(FULL, gA_c2, 1);
 }
 
+// Copy what the y lines c0 .. c0+7 read (state, material and adjoint of their
+// columns and of the two next to them, rows j0-3 .. j0+AT+2) into STG with
+// row-wise loads; a y line's lanes then read down a column of STG (odd pitch:
+// no bank conflicts) instead of with a row-pitch stride from global memory.
+// Cells outside the ghosted array are set to 0 (no lane reads them).
+__device__ __forceinline__ void adj_stage_y(const AdjArgs& a, const double* __restrict__ q,
+                                            const double* __restrict__ lin, double* STG, int c0, int j0)
+{
+    constexpr int NC = ANT / 32 + 2;
+    const int n = YF * YR * NC;
+    for (int t = threadIdx.x; t < n; t += ANT) {
+        const int f = t / (YR * NC), rem = t % (YR * NC);
+        const int r = rem / NC, c = rem % NC;
+        const int col = c0 - 1 + c, row = j0 - 3 + r;
+        double v = 0.0;
+        if (col >= -CLAW2_NUM_GHOST && col < a.mx + CLAW2_NUM_GHOST && row >= -CLAW2_NUM_GHOST &&
+            row < a.my + CLAW2_NUM_GHOST) {
+            const long long o = cell(a, col, row);
+            switch (f) {
+            case 0: v = q[o]; break;
+            case 1: v = q[o + 2 * a.plane]; break;
+            case 2: v = a.aux[o]; break;
+            case 3: v = a.aux[o + a.plane]; break;
+            case 4: v = lin[o]; break;
+            case 5: v = lin[o + a.plane]; break;
+            default: v = lin[o + 2 * a.plane]; break;
+            }
+        }
+        STG[(f * YR + r) * YP + c] = v;
+    }
+}
+
 // One sweep direction of a tile: lines first..last in chunks of 8 (one per
 // warp).  Each chunk stages its lines' aux gradients for the neighbouring
 // lines (up, dn) in one half of XS, passes one barrier, and then every line
@@ -342,7 +393,7 @@ __device__ __forceinline__ void adj_line(const AdjArgs& a, const double* __restr
 template <int IXY>
 __device__ __forceinline__ void adj_sweep(const AdjArgs& a, const double* __restrict__ q,
                                           const double* __restrict__ lin, int i0, int j0, int ilo, int ihi, int jlo,
-                                          int jhi, double* GQ, double* GA, double* XS, int& chunk)
+                                          int jhi, double* GQ, double* GA, double* XS, double* STG, int& chunk)
 {
     constexpr int MN = IXY == 1 ? 1 : 2;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -360,8 +411,13 @@ __device__ __forceinline__ void adj_sweep(const AdjArgs& a, const double* __rest
         const int clast = c0 + ANT / 32 - 1 < last ? c0 + ANT / 32 - 1 : last;
         const bool ok = line <= last;
         const bool own = ok && line >= llo && line < lhi;
+        if constexpr (IXY == 2) {
+            // the previous chunk's barrier has passed: no lane still reads STG
+            adj_stage_y(a, q, lin, STG, c0, j0);
+            __syncthreads();
+        }
         LineOut o;
-        adj_line<IXY>(a, q, lin, i0, j0, line, ok, own, o);
+        adj_line<IXY>(a, q, lin, STG, line - c0 + 1, i0, j0, line, ok, own, o);
         const int c = (IXY == 1 ? i0 : j0) - 2 + lane;
         const bool cown = ok && c >= clo && c < chi;
         double* X = XS + (chunk & 1) * 4 * ANT;
@@ -404,6 +460,7 @@ __global__ void __launch_bounds__(ANT, CLAW2_ADJ_MINB) adjoint_kernel(AdjArgs a)
     double* GQ = adj_smem;                    // 3 x AR x AR state adjoint
     double* GA = GQ + 3 * AR * AR;            // 2 x AR x AR aux gradient
     double* XS = GA + 2 * AR * AR;            // 2 x 4 x ANT cross-line exchange
+    double* STG = XS + 2 * 4 * ANT;           // YF x YR x YP staged inputs of a chunk of y lines
     const int shot = blockIdx.z;
     const double* __restrict__ q = a.q + shot * a.qstride;
     const double* __restrict__ lin = a.lam_in + shot * a.qstride;
@@ -427,8 +484,8 @@ __global__ void __launch_bounds__(ANT, CLAW2_ADJ_MINB) adjoint_kernel(AdjArgs a)
     }
     __syncthreads();
     int chunk = 0;
-    adj_sweep<1>(a, q, lin, i0, j0, ilo, ihi, jlo, jhi, GQ, GA, XS, chunk);     // x-slices: rows
-    adj_sweep<2>(a, q, lin, i0, j0, ilo, ihi, jlo, jhi, GQ, GA, XS, chunk);     // y-slices: columns
+    adj_sweep<1>(a, q, lin, i0, j0, ilo, ihi, jlo, jhi, GQ, GA, XS, STG, chunk);     // x-slices: rows
+    adj_sweep<2>(a, q, lin, i0, j0, ilo, ihi, jlo, jhi, GQ, GA, XS, STG, chunk);     // y-slices: columns
     __syncthreads();
 
     for (int t = tid; t < AR * AR; t += ANT) {
@@ -687,7 +744,7 @@ int claw2_shots_adjoint_step(const claw2_problem* p, int nshots, long long shot_
     a.dtdx = dt / p->dx; a.dtdy = dt / p->dy;
     a.order = p->order; a.trans = p->transverse;
     a.mthlim[0] = p->mthlim[0]; a.mthlim[1] = p->mthlim[1];
-    constexpr int smem = (5 * AR * AR + 2 * 4 * ANT) * 8;
+    constexpr int smem = (5 * AR * AR + 2 * 4 * ANT + YF * YR * YP) * 8;
     static bool configured = false;
     if (!configured) {
         if (cudaFuncSetAttribute(adjoint_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)

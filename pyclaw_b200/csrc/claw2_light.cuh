@@ -83,21 +83,57 @@ template <> struct LightOf<RpAcoustics> { using type = LightAcoustics; };
 template <> struct LightOf<RpVcAcoustics> { using type = LightVcAcoustics; };
 
 // shared memory of the light body (doubles): the tile state, the cross-line
-// exchange (2 buffers x 4 values x NT) and the reduction scratch
+// exchange (2 buffers x 4 values x NT), the reduction scratch and the staged
+// inputs of one chunk of y lines (4 fields x YR rows x YP columns)
 template <int TX, int TY, int NT> struct LightSmem {
     static constexpr int QX = 3 * TX * TY;
     static constexpr int CX = 2 * 4 * NT;
-    static constexpr int total = QX + CX + NT;
+    static constexpr int YR = TY + 4;            // rows j0-2 .. j0+TY+1 read by the lanes
+    static constexpr int YP = NT / 32 + 3;       // columns c0-1 .. c0+LPC, padded to an odd pitch
+    static constexpr int YS = 4 * YR * YP;
+    static constexpr int total = QX + CX + NT + YS;
     static constexpr int bytes = total * 8;
 };
+
+// Copy what the y lines c0 .. c0+LPC-1 read (pressure and y-velocity of their
+// columns, (rho, c) of those columns and the two next to them) into STG with
+// row-wise (coalesced) loads.  Each lane of a y line reads down a column, which
+// in global memory is a row-pitch stride per lane; in STG the pitch YP is odd,
+// so those reads are free of bank conflicts.  Cells outside the ghosted array
+// are set to 0 (no lane reads them).
+template <int TY, int NT, bool VC, class Ctx>
+CLAW2_HD void light_stage_y(const StepArgs& a, Ctx& ctx, const double* __restrict__ qin, double* STG, int c0, int j0)
+{
+    constexpr int YR = TY + 4, YP = NT / 32 + 3, NC = NT / 32 + 2;
+    constexpr int NF = VC ? 4 : 2;
+    const int n = NF * YR * NC;
+    for (int t = ctx.tid(); t < n; t += NT) {
+        const int f = t / (YR * NC), rem = t % (YR * NC);
+        const int r = rem / NC, c = rem % NC;
+        const int col = c0 - 1 + c, row = j0 - 2 + r;
+        double v = 0.0;
+        if (col >= -CLAW2_NUM_GHOST && col < a.mx + CLAW2_NUM_GHOST && row >= -CLAW2_NUM_GHOST &&
+            row < a.my + CLAW2_NUM_GHOST) {
+            const long long o = qoff(a, 0, col, row);
+            if (f == 0) v = qin[o];
+            else if (f == 1) v = qin[o + 2 * a.plane];
+            else v = a.aux[o + (f - 2) * a.plane];
+        }
+        STG[(f * YR + r) * YP + c] = v;
+    }
+}
 
 // One chunk of one sweep direction (see sweep_chunk for the meaning of the
 // arguments).  buf selects the half of the exchange array this chunk uses.
 template <class LRP, int IXY, int TX, int TY, int NT, class Ctx>
 CLAW2_HD void light_chunk(const StepArgs& a, Ctx& ctx, const double* __restrict__ qin, double* Qx, double* CXb,
-                          int i0, int j0, int line, int cfirst, int clast, bool lineok, double dtn, double dtt,
-                          double& cflm)
+                          const double* STG, int i0, int j0, int line, int cfirst, int clast, bool lineok,
+                          double dtn, double dtt, double& cflm)
 {
+    // y lines read their inputs from the staged copy: field f, row r (= the
+    // lane's left cell k-1 at r = slot), column c (= line at c = line-cfirst+1)
+    constexpr int YR = TY + 4, YP = NT / 32 + 3;
+    auto stg = [&](int f, int r, int c) -> double { return STG[(f * YR + r) * YP + c]; };
     constexpr int MU = IXY == 1 ? 1 : 2, MV = IXY == 1 ? 2 : 1;
     constexpr int NCELL = IXY == 1 ? TX : TY;
     constexpr int NSLOT = NCELL + 3;
@@ -114,14 +150,24 @@ CLAW2_HD void light_chunk(const StepArgs& a, Ctx& ctx, const double* __restrict_
 
     // ---------------- normal solve ----------------
     double w1p = 0.0, w1n = 0.0, s1 = 0.0, w2p = 0.0, w2n = 0.0, s2 = 0.0;
+    const int sc = line - cfirst + 1;                 // this line's column in STG (y lines)
     if (ifok) {
         double auxL[2] = {0.0, 0.0}, auxR[2] = {0.0, 0.0};
-        if (LRP::VC) {
-            auxL[0] = a.aux[oL]; auxL[1] = a.aux[oL + P];
-            auxR[0] = a.aux[oR]; auxR[1] = a.aux[oR + P];
+        if constexpr (IXY == 2) {
+            if (LRP::VC) {
+                auxL[0] = stg(2, slot, sc); auxL[1] = stg(3, slot, sc);
+                auxR[0] = stg(2, slot + 1, sc); auxR[1] = stg(3, slot + 1, sc);
+            }
+            LRP::rpn2(stg(0, slot, sc), stg(1, slot, sc), stg(0, slot + 1, sc), stg(1, slot + 1, sc), auxL, auxR,
+                      a.prm, w1p, w1n, s1, w2p, w2n, s2);
+        } else {
+            if (LRP::VC) {
+                auxL[0] = a.aux[oL]; auxL[1] = a.aux[oL + P];
+                auxR[0] = a.aux[oR]; auxR[1] = a.aux[oR + P];
+            }
+            LRP::rpn2(qin[oL], qin[oL + MU * P], qin[oR], qin[oR + MU * P], auxL, auxR, a.prm, w1p, w1n, s1, w2p,
+                      w2n, s2);
         }
-        LRP::rpn2(qin[oL], qin[oL + MU * P], qin[oR], qin[oR + MU * P], auxL, auxR, a.prm, w1p, w1n, s1, w2p,
-                  w2n, s2);
     }
     const double l1p = ctx.shfl_up(w1p), l1n = ctx.shfl_up(w1n), l2p = ctx.shfl_up(w2p), l2n = ctx.shfl_up(w2n);
     const double r1p = ctx.shfl_down(w1p), r1n = ctx.shfl_down(w1n);
@@ -181,15 +227,27 @@ CLAW2_HD void light_chunk(const StepArgs& a, Ctx& ctx, const double* __restrict_
             const double Pf = cor ? apdq_p - cq_p : apdq_p;
             double ax1[2] = {0.0, 0.0}, ax2[2] = {0.0, 0.0}, ax3[2] = {0.0, 0.0};
             if (LRP::VC) {
-                ax1[0] = a.aux[oL - across]; ax1[1] = a.aux[oL - across + P];
-                ax2[0] = a.aux[oL]; ax2[1] = a.aux[oL + P];
-                ax3[0] = a.aux[oL + across]; ax3[1] = a.aux[oL + across + P];
+                if constexpr (IXY == 2) {
+                    ax1[0] = stg(2, slot, sc - 1); ax1[1] = stg(3, slot, sc - 1);
+                    ax2[0] = stg(2, slot, sc); ax2[1] = stg(3, slot, sc);
+                    ax3[0] = stg(2, slot, sc + 1); ax3[1] = stg(3, slot, sc + 1);
+                } else {
+                    ax1[0] = a.aux[oL - across]; ax1[1] = a.aux[oL - across + P];
+                    ax2[0] = a.aux[oL]; ax2[1] = a.aux[oL + P];
+                    ax3[0] = a.aux[oL + across]; ax3[1] = a.aux[oL + across + P];
+                }
             }
             LRP::rpt2(A, ax1, ax2, ax3, a.prm, bmL_p, bmL_t, bpL_p, bpL_t);
             if (LRP::VC) {
-                ax1[0] = a.aux[oR - across]; ax1[1] = a.aux[oR - across + P];
-                ax2[0] = a.aux[oR]; ax2[1] = a.aux[oR + P];
-                ax3[0] = a.aux[oR + across]; ax3[1] = a.aux[oR + across + P];
+                if constexpr (IXY == 2) {
+                    ax1[0] = stg(2, slot + 1, sc - 1); ax1[1] = stg(3, slot + 1, sc - 1);
+                    ax2[0] = stg(2, slot + 1, sc); ax2[1] = stg(3, slot + 1, sc);
+                    ax3[0] = stg(2, slot + 1, sc + 1); ax3[1] = stg(3, slot + 1, sc + 1);
+                } else {
+                    ax1[0] = a.aux[oR - across]; ax1[1] = a.aux[oR - across + P];
+                    ax2[0] = a.aux[oR]; ax2[1] = a.aux[oR + P];
+                    ax3[0] = a.aux[oR + across]; ax3[1] = a.aux[oR + across + P];
+                }
             }
             LRP::rpt2(Pf, ax1, ax2, ax3, a.prm, bmR_p, bmR_t, bpR_p, bpR_t);
         }
@@ -301,6 +359,7 @@ CLAW2_HD void light_tile_at(const StepArgs& a, Ctx& ctx, const TileId& tile)
     double* Qx = ctx.smem();
     double* CX = Qx + SM::QX;
     double* red = CX + SM::CX;
+    double* STG = red + NT;
     const int tid = ctx.tid();
     const int warp = tid >> 5;
     const int i0 = tile.bx * TX, j0 = tile.by * TY;
@@ -323,8 +382,8 @@ CLAW2_HD void light_tile_at(const StepArgs& a, Ctx& ctx, const TileId& tile)
         for (int c0 = first; c0 <= last; c0 += LPC, chunk++) {
             const int line = c0 + warp;
             const int clast = (c0 + LPC - 1 < last) ? c0 + LPC - 1 : last;
-            light_chunk<LRP, 1, TX, TY, NT>(a, ctx, qin, Qx, CX + (chunk & 1) * 4 * NT, i0, j0, line, c0, clast,
-                                            line <= last, dtdx, dtdy, cflm);
+            light_chunk<LRP, 1, TX, TY, NT>(a, ctx, qin, Qx, CX + (chunk & 1) * 4 * NT, nullptr, i0, j0, line, c0,
+                                            clast, line <= last, dtdx, dtdy, cflm);
         }
     }
     {
@@ -333,8 +392,11 @@ CLAW2_HD void light_tile_at(const StepArgs& a, Ctx& ctx, const TileId& tile)
         for (int c0 = first; c0 <= last; c0 += LPC, chunk++) {
             const int line = c0 + warp;
             const int clast = (c0 + LPC - 1 < last) ? c0 + LPC - 1 : last;
-            light_chunk<LRP, 2, TX, TY, NT>(a, ctx, qin, Qx, CX + (chunk & 1) * 4 * NT, i0, j0, line, c0, clast,
-                                            line <= last, dtdy, dtdx, cflm);
+            // the previous chunk's barrier has passed: no lane still reads STG
+            light_stage_y<TY, NT, LRP::VC>(a, ctx, qin, STG, c0, j0);
+            ctx.sync();
+            light_chunk<LRP, 2, TX, TY, NT>(a, ctx, qin, Qx, CX + (chunk & 1) * 4 * NT, STG, i0, j0, line, c0,
+                                            clast, line <= last, dtdy, dtdx, cflm);
         }
     }
     ctx.sync();
