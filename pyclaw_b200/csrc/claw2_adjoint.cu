@@ -359,27 +359,22 @@ __device__ __forceinline__ void adj_line(const AdjArgs& a, const double* __restr
 __device__ __forceinline__ void adj_stage_y(const AdjArgs& a, const double* __restrict__ q,
                                             const double* __restrict__ lin, double* STG, int c0, int j0)
 {
-    constexpr int NC = ANT / 32 + 2;
-    const int n = YF * YR * NC;
-    for (int t = threadIdx.x; t < n; t += ANT) {
-        const int f = t / (YR * NC), rem = t % (YR * NC);
-        const int r = rem / NC, c = rem % NC;
+    constexpr int NC = ANT / 32 + 2, NPOS = YR * NC, FS = YR * YP;
+    const long long P = a.plane;
+    for (int t = threadIdx.x; t < NPOS; t += ANT) {      // positions once, then every field
+        const int r = t / NC, c = t - r * NC;
         const int col = c0 - 1 + c, row = j0 - 3 + r;
-        double v = 0.0;
-        if (col >= -CLAW2_NUM_GHOST && col < a.mx + CLAW2_NUM_GHOST && row >= -CLAW2_NUM_GHOST &&
-            row < a.my + CLAW2_NUM_GHOST) {
-            const long long o = cell(a, col, row);
-            switch (f) {
-            case 0: v = q[o]; break;
-            case 1: v = q[o + 2 * a.plane]; break;
-            case 2: v = a.aux[o]; break;
-            case 3: v = a.aux[o + a.plane]; break;
-            case 4: v = lin[o]; break;
-            case 5: v = lin[o + a.plane]; break;
-            default: v = lin[o + 2 * a.plane]; break;
-            }
-        }
-        STG[(f * YR + r) * YP + c] = v;
+        const bool in = col >= -CLAW2_NUM_GHOST && col < a.mx + CLAW2_NUM_GHOST && row >= -CLAW2_NUM_GHOST &&
+                        row < a.my + CLAW2_NUM_GHOST;
+        const long long o = in ? cell(a, col, row) : 0;
+        double* d = STG + r * YP + c;
+        d[0 * FS] = in ? q[o] : 0.0;
+        d[1 * FS] = in ? q[o + 2 * P] : 0.0;
+        d[2 * FS] = in ? a.aux[o] : 0.0;
+        d[3 * FS] = in ? a.aux[o + P] : 0.0;
+        d[4 * FS] = in ? lin[o] : 0.0;
+        d[5 * FS] = in ? lin[o + P] : 0.0;
+        d[6 * FS] = in ? lin[o + 2 * P] : 0.0;
     }
 }
 

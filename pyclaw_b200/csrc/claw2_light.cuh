@@ -104,22 +104,21 @@ template <int TX, int TY, int NT> struct LightSmem {
 template <int TY, int NT, bool VC, class Ctx>
 CLAW2_HD void light_stage_y(const StepArgs& a, Ctx& ctx, const double* __restrict__ qin, double* STG, int c0, int j0)
 {
-    constexpr int YR = TY + 4, YP = NT / 32 + 3, NC = NT / 32 + 2;
-    constexpr int NF = VC ? 4 : 2;
-    const int n = NF * YR * NC;
-    for (int t = ctx.tid(); t < n; t += NT) {
-        const int f = t / (YR * NC), rem = t % (YR * NC);
-        const int r = rem / NC, c = rem % NC;
+    constexpr int YR = TY + 4, YP = NT / 32 + 3, NC = NT / 32 + 2, NPOS = YR * NC, FS = YR * YP;
+    const long long P = a.plane;
+    for (int t = ctx.tid(); t < NPOS; t += NT) {          // positions once, then every field
+        const int r = t / NC, c = t - r * NC;
         const int col = c0 - 1 + c, row = j0 - 2 + r;
-        double v = 0.0;
-        if (col >= -CLAW2_NUM_GHOST && col < a.mx + CLAW2_NUM_GHOST && row >= -CLAW2_NUM_GHOST &&
-            row < a.my + CLAW2_NUM_GHOST) {
-            const long long o = qoff(a, 0, col, row);
-            if (f == 0) v = qin[o];
-            else if (f == 1) v = qin[o + 2 * a.plane];
-            else v = a.aux[o + (f - 2) * a.plane];
+        const bool in = col >= -CLAW2_NUM_GHOST && col < a.mx + CLAW2_NUM_GHOST && row >= -CLAW2_NUM_GHOST &&
+                        row < a.my + CLAW2_NUM_GHOST;
+        const long long o = in ? qoff(a, 0, col, row) : 0;
+        double* d = STG + r * YP + c;
+        d[0 * FS] = in ? qin[o] : 0.0;
+        d[1 * FS] = in ? qin[o + 2 * P] : 0.0;
+        if (VC) {
+            d[2 * FS] = in ? a.aux[o] : 0.0;
+            d[3 * FS] = in ? a.aux[o + P] : 0.0;
         }
-        STG[(f * YR + r) * YP + c] = v;
     }
 }
 
