@@ -235,6 +235,43 @@ CLAW2_EXPORT int claw2_advance_hooked(const claw2_problem* p, double* q0, double
                                       claw2_control* ctrl, void* scratch, int nsteps, const claw2_hooks* hooks,
                                       void* stream);
 
+/* ---- domain decomposition: one slab of a larger grid per process -------- */
+/* The reference runs one grid per process under PETSc (PetClaw: a DA with a
+ * halo exchange, src/petclaw/state.py:268, and a global CFL max,
+ * src/petclaw/cfl.py:30-31).  Here a slab is a claw2_problem whose sides that
+ * face another slab are custom (bc 0); per step every slab runs, in order:
+ * claw2_halo_pack (its two boundary rows of q[cur] into a buffer),
+ * the exchange of those buffers between neighbours (the caller's transport,
+ * e.g. NCCL), claw2_halo_unpack (the neighbours' rows into the ghost rows),
+ * claw2_step_ctrl, a max-reduction of the CFL numbers over all slabs (the
+ * caller's transport), claw2_control_apply and claw2_fill_ghosts_ctrl.  All of
+ * it is asynchronous on the stream; cur and dt are read on the device. */
+
+/* One step q[cur] -> q[1-cur] with dt and cur read from ctrl (as
+ * claw2_advance), writing the slab's CFL number to cfl_dev (+inf when the new
+ * state is not finite) and leaving ctrl unchanged.  Ghost cells of the new
+ * state are not written; fill them with claw2_fill_ghosts_ctrl after
+ * claw2_control_apply. */
+CLAW2_EXPORT int claw2_step_ctrl(const claw2_problem* p, double* q0, double* q1, const double* aux,
+                                 claw2_control* ctrl, void* scratch, double* cfl_dev, void* stream);
+
+/* One iteration of the controller (as claw2_advance's) with the CFL number
+ * *cfl_dev (a max over all slabs; +inf or NaN: non-finite state). */
+CLAW2_EXPORT int claw2_control_apply(claw2_control* ctrl, const double* cfl_dev, void* stream);
+
+/* Ghost fill (claw2_fill_ghosts) of q[ctrl->cur]; custom sides untouched. */
+CLAW2_EXPORT int claw2_fill_ghosts_ctrl(const claw2_problem* p, double* q0, double* q1, const claw2_control* ctrl,
+                                        void* stream);
+
+/* Halo rows of q[ctrl->cur], all components and all columns including the
+ * ghost columns, as num_eqn x 2 x (mx+4) doubles (component, row, column).
+ * pack: upper = 0 the rows 0,1, upper = 1 the rows my-2,my-1;
+ * unpack: upper = 0 into the ghost rows -2,-1, upper = 1 into my,my+1. */
+CLAW2_EXPORT int claw2_halo_pack(const claw2_problem* p, const double* q0, const double* q1,
+                                 const claw2_control* ctrl, int upper, double* buf, void* stream);
+CLAW2_EXPORT int claw2_halo_unpack(const claw2_problem* p, double* q0, double* q1, const claw2_control* ctrl,
+                                   int upper, const double* buf, void* stream);
+
 /* Host-side initialisation of a controller for evolve_to_time(solution, tend)
  * (solver.py:600-641): status reset, fixed-dt step count, first clamp. */
 CLAW2_EXPORT int claw2_control_init(claw2_control* c, double t, double dt, double tend,

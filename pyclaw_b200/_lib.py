@@ -34,6 +34,11 @@ PROTOTYPES = [
     ("claw2_advance", ctypes.c_int, [_P, _dp, _dp, _dp, _vp, _vp, ctypes.c_int, _vp]),
     ("claw2_advance_hooked", ctypes.c_int, [_P, _dp, _dp, _dp, _vp, _vp, ctypes.c_int, ctypes.POINTER(_abi.Hooks),
                                             _vp]),
+    ("claw2_step_ctrl", ctypes.c_int, [_P, _dp, _dp, _dp, _vp, _vp, _dp, _vp]),
+    ("claw2_control_apply", ctypes.c_int, [_vp, _dp, _vp]),
+    ("claw2_fill_ghosts_ctrl", ctypes.c_int, [_P, _dp, _dp, _vp, _vp]),
+    ("claw2_halo_pack", ctypes.c_int, [_P, _dp, _dp, _vp, ctypes.c_int, _dp, _vp]),
+    ("claw2_halo_unpack", ctypes.c_int, [_P, _dp, _dp, _vp, ctypes.c_int, _dp, _vp]),
     ("claw2_control_init", ctypes.c_int, [_C, _dbl, _dbl, _dbl, _dbl, _dbl, _dbl, ctypes.c_int,
                                           ctypes.c_int, _i64, _dbl]),
     ("claw2_ref_to_device", ctypes.c_int, [_P, ctypes.c_int, _dp, _dp, _vp]),

@@ -182,6 +182,32 @@ __global__ void dev_to_ref_kernel(const double* dev, double* ref, int nc, int nx
     }
 }
 
+// domain decomposition helpers: controller update from a given CFL number,
+// and the two halo rows of q[cur] to/from a contiguous buffer
+__global__ void control_apply_kernel(claw2_control* c, const double* cfl)
+{
+    const double v = *cfl;
+    const bool nonfinite = !(v < 1.0 / 0.0);          // +inf or NaN
+    if (!c->done) control_update(c, nonfinite ? 0.0 : v, nonfinite ? 1 : 0);
+}
+
+__global__ void halo_kernel(double* q0, double* q1, const claw2_control* c, double* buf, long long ld,
+                            long long plane, int mx, int my, int ncomp, int upper, int unpack)
+{
+    double* q = c->cur ? q1 : q0;
+    const int w = mx + 2 * CLAW2_NUM_GHOST;
+    const int total = ncomp * 2 * w;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+        const int i = t % w - CLAW2_NUM_GHOST, r = (t / w) % 2, m = t / (2 * w);
+        int row;
+        if (!unpack) row = upper ? my - 2 + r : r;
+        else row = upper ? my + r : -2 + r;
+        const long long o = (long long)m * plane + (long long)(row + CLAW2_NUM_GHOST) * ld + (i + CLAW2_NUM_GHOST);
+        if (unpack) q[o] = buf[t];
+        else buf[t] = q[o];
+    }
+}
+
 }  // namespace claw2
 
 using namespace claw2;
@@ -489,6 +515,64 @@ int claw2_advance_hooked(const claw2_problem* p, double* q0, double* q1, const d
             return rc;
     }
     return CLAW2_OK;
+}
+
+int claw2_step_ctrl(const claw2_problem* p, double* q0, double* q1, const double* aux, claw2_control* ctrl,
+                    void* scratch, double* cfl_dev, void* stream)
+{
+    int rc = claw2_validate(p);
+    if (rc) return rc;
+    if (!q0 || !q1 || !ctrl || !scratch || !cfl_dev || (p->num_aux > 0 && !aux)) return CLAW2_ERR_INVALID;
+    StepArgs a;
+    fill_args(p, q0, a);
+    a.q0 = q0; a.q1 = q1; a.aux = aux; a.ctrl = ctrl;
+    a.ctrl_readonly = 1;
+    a.cfl_out = cfl_dev;
+    a.ghost_fused = 0;
+    a.ticket = static_cast<unsigned int*>(scratch);
+    a.partials = reinterpret_cast<double*>(static_cast<char*>(scratch) + 64);
+    return launch_step(p, a, S(stream));
+}
+
+int claw2_control_apply(claw2_control* ctrl, const double* cfl_dev, void* stream)
+{
+    if (!ctrl || !cfl_dev) return CLAW2_ERR_INVALID;
+    control_apply_kernel<<<1, 1, 0, S(stream)>>>(ctrl, cfl_dev);
+    return cudaGetLastError() == cudaSuccess ? CLAW2_OK : CLAW2_ERR_CUDA;
+}
+
+int claw2_fill_ghosts_ctrl(const claw2_problem* p, double* q0, double* q1, const claw2_control* ctrl, void* stream)
+{
+    int rc = claw2_validate(p);
+    if (rc) return rc;
+    if (!q0 || !q1 || !ctrl) return CLAW2_ERR_INVALID;
+    return launch_fill(p, nullptr, p->num_eqn, p->bc_lower, p->bc_upper, false, q0, q1, ctrl, S(stream));
+}
+
+static int halo(const claw2_problem* p, double* q0, double* q1, const claw2_control* ctrl, int upper, double* buf,
+                int unpack, void* stream)
+{
+    int rc = claw2_validate(p);
+    if (rc) return rc;
+    if (!q0 || !q1 || !ctrl || !buf || (upper != 0 && upper != 1) || p->my < 2) return CLAW2_ERR_INVALID;
+    claw2_layout L;
+    claw2_get_layout(p, &L);
+    const int total = p->num_eqn * 2 * (p->mx + 2 * CLAW2_NUM_GHOST);
+    halo_kernel<<<(total + 255) / 256, 256, 0, S(stream)>>>(q0, q1, ctrl, buf, L.ld, L.plane, p->mx, p->my,
+                                                           p->num_eqn, upper, unpack);
+    return cudaGetLastError() == cudaSuccess ? CLAW2_OK : CLAW2_ERR_CUDA;
+}
+
+int claw2_halo_pack(const claw2_problem* p, const double* q0, const double* q1, const claw2_control* ctrl, int upper,
+                    double* buf, void* stream)
+{
+    return halo(p, const_cast<double*>(q0), const_cast<double*>(q1), ctrl, upper, buf, 0, stream);
+}
+
+int claw2_halo_unpack(const claw2_problem* p, double* q0, double* q1, const claw2_control* ctrl, int upper,
+                      const double* buf, void* stream)
+{
+    return halo(p, q0, q1, ctrl, upper, const_cast<double*>(buf), 1, stream);
 }
 
 int claw2_control_init(claw2_control* c, double t, double dt, double tend, double cfl_max, double cfl_desired,

@@ -55,6 +55,8 @@ struct StepArgs {
     int ghost_fused;
     int bcl[2], bcu[2];
     int src, src_aux;      // source term fused into the final write (claw2_source)
+    int ctrl_readonly;     // controlled mode that reports the CFL (cfl_out, +inf if
+                           // non-finite) instead of updating ctrl (domain decomposition)
 };
 
 template <int IXY> struct Phase;
@@ -595,7 +597,8 @@ CLAW2_HD void finish_tile(const StepArgs& a, Ctx& ctx, const TileId& tile, const
                 if (v < 0.0) nonfinite = 1;
                 else cfl = cfl > v ? cfl : v;
             }
-            if (a.ctrl) control_update(a.ctrl, cfl, nonfinite);
+            if (a.ctrl && !a.ctrl_readonly) control_update(a.ctrl, cfl, nonfinite);
+            else if (a.ctrl_readonly) *a.cfl_out = nonfinite ? 1.0 / 0.0 : cfl;
             else *a.cfl_out = nonfinite ? ctx.nan() : cfl;
             *a.ticket = 0u;
             ctx.fence();
