@@ -689,6 +689,59 @@ def run_shallow(args):
     print(json.dumps(line), flush=True)
 
 
+def run_acoustics(args):
+    """Config 1: 256^2 constant-coefficient acoustics (walls, unsplit with
+    transverse_waves=2, MC, cfl_desired 0.9) from t = 0 to 0.6 through the
+    device-controlled loop (one launch per step, the light tile body); the
+    whole run is timed with CUDA events, the oracle's OpenMP form times the
+    same run on the host cores."""
+    import torch
+    from pyclaw_b200 import _abi, _lib
+    from pyclaw_b200.device import DeviceState
+    lib = _lib.load()
+    prob, q, aux, run, tfinal = acoustics_config()
+    cells = prob.mx * prob.my
+    dev = DeviceState(prob, torch.device("cuda"))
+
+    def once():
+        dev.upload_q(q)
+        dev.cur = 0
+        c = _abi.Control()
+        _lib.check(lib.claw2_control_init(ctypes.byref(c), 0.0, run["dt_initial"], tfinal, run["cfl_max"],
+                                          run["cfl_desired"], 1e99, 1, 0, 1 << 40, run["cfl_desired"]),
+                   "claw2_control_init")
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        out = dev.evolve(c)
+        e1.record()
+        torch.cuda.synchronize()
+        return out, e0.elapsed_time(e1) / 1e3
+
+    for _ in range(max(1, args.warmup // 3)):
+        once()
+    out, t = once()
+    if out.error:
+        raise RuntimeError("device loop error %d" % out.error)
+    value = out.numsteps * cells / t
+    cpu = None
+    if not args.no_cpu:
+        rate, n, thr, el = cpu_rate(prob, q, run, omp=True, max_seconds=8.0)
+        cpu = {"value": rate, "unit": "cell-updates/s", "cores": thr, "kind": "port",
+               "sample": "%d whole-grid steps (%.1f s) of the 256^2 acoustics run, oracle OpenMP gather form, "
+                         "%d threads" % (n, el, thr)}
+    line = {
+        "metric": "cell_updates_per_s", "value": value, "unit": "cell-updates/s", "n_gpus": 1,
+        "steps": int(out.numsteps), "ms_per_step": t / out.numsteps * 1e3, "higher_is_better": True,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "acoustics_256x256_walls_t0.6", "solver": "acoustics", "limiter": "MC",
+                   "transverse_waves": 2, "t_final": out.t, "run_seconds": t,
+                   "timing": "whole run to t=0.6 incl. the host polling of the controller every batch of steps"},
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def run_adjoint(args):
     """The adjoint workload: traces of `shots` shots over `nsteps` steps for the
     starting material, the L2 misfit against the target material's traces,
@@ -772,7 +825,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--workload", default="shockbubble", choices=["shockbubble", "batched", "adjoint", "shallow"])
+    ap.add_argument("--workload", default="shockbubble", choices=["shockbubble", "batched", "adjoint", "shallow", "acoustics"])
     ap.add_argument("--sw-n", type=int, default=4096)
     ap.add_argument("--sw-steps", type=int, default=500)
     ap.add_argument("--instances", type=int, default=1024)
@@ -791,6 +844,9 @@ def main():
         elif args.workload == "shallow":
             if rank == 0:
                 run_shallow(args)
+        elif args.workload == "acoustics":
+            if rank == 0:
+                run_acoustics(args)
         elif args.impl == "reference":
             run_reference_arm(args, world, rank)
         else:
