@@ -513,8 +513,11 @@ def run_ours(args, world, rank, local):
                          "peak_source": peak_kind,
                          "algorithmic_bytes_per_launch": alg_bytes},
             "cpu_baseline": cpu,
+            # one call = one output interval of Controller.run: the state goes up
+            # once, the steps of the interval run on the device, the state comes back
             "e2e": {"value": e2e_val, "unit": "cell-updates/s",
-                    "h2d_bytes_per_step": e2e["h2d"], "d2h_bytes_per_step": e2e["d2h"],
+                    "h2d_bytes_per_step": e2e["h2d"] / e2e["steps"], "d2h_bytes_per_step": e2e["d2h"] / e2e["steps"],
+                    "h2d_bytes_per_call": e2e["h2d"], "d2h_bytes_per_call": e2e["d2h"],
                     "steps_per_call": e2e["steps"], "calls": e2e["calls"]} if e2e else None,
             "gpu_launches": int(args.steps),
             "clocks": clk,
