@@ -102,7 +102,7 @@ CLAW2_HD double philim(double a, double b, int meth, DV& dv)
 
 CLAW2_HD double philim(double a, double b, int meth)
 {
-    IeeeDiv d;
+    IeeeRn d;
     return philim(a, b, meth, d);
 }
 
@@ -705,16 +705,16 @@ CLAW2_HD void step_tile_at(const StepArgs& a, Ctx& ctx, const TileId& tile)
     double cflm = 0.0;
 #if defined(__CUDA_ARCH__)
     // The sweeps rebuild Qx from qin alone, so a tile can be redone: with
-    // IEEE division when a FastDiv quotient was not proven correctly rounded.
-    FastDiv f;
+    // IEEE division when a FastRn quotient was not proven correctly rounded.
+    FastRn f;
     tile_sweeps<RP, TX, TY, NT, SPLIT>(a, ctx, qin, Qx, WB, B2, i0, j0, dtdx, dtdy, cflm, f);
     if (__syncthreads_or(!f.ok)) {
-        IeeeDiv d;
+        IeeeRn d;
         cflm = 0.0;
         tile_sweeps<RP, TX, TY, NT, SPLIT>(a, ctx, qin, Qx, WB, B2, i0, j0, dtdx, dtdy, cflm, d);
     }
 #else
-    IeeeDiv d;
+    IeeeRn d;
     tile_sweeps<RP, TX, TY, NT, SPLIT>(a, ctx, qin, Qx, WB, B2, i0, j0, dtdx, dtdy, cflm, d);
 #endif
     finish_tile<MEQN, TX, TY, NT>(a, ctx, tile, Qx + (-QROW0) * TX, QROWS * TX, red, qout, i0, j0, cflm, dt);

@@ -12,10 +12,11 @@
 // --fmad=false), so results agree bit for bit with the CPU oracle except for
 // the sign of exact zeros where a structurally zero term is skipped.
 //
-// Divisions go through the policy object dv (claw2_fastdiv.cuh): FastDiv
-// computes the correctly rounded quotient without a slow-path branch, or flags
-// that it could not prove it; the tile kernel then redoes the tile with
-// IeeeDiv, so every result is the IEEE quotient's.
+// Divisions and square roots go through the policy object dv
+// (claw2_fastrn.cuh): dv(a, b) = a/b, dv.sqrt(x).  FastRn computes the
+// correctly rounded result without a slow-path branch, or flags that it could
+// not prove it; the tile kernel then redoes the tile with IeeeRn, so every
+// result is the IEEE one.
 //
 // Indexing: qL is the cell left of the interface (Fortran qr(:,i-1)), qR the
 // cell right of it (Fortran ql(:,i)).  IXY = 1 for x slices, 2 for y slices;
@@ -24,7 +25,7 @@
 
 #if defined(__CUDACC__)
 #define CLAW2_DEV __device__ __forceinline__
-#include "claw2_fastdiv.cuh"
+#include "claw2_fastrn.cuh"
 #else
 #include <cmath>
 #define CLAW2_DEV inline
@@ -57,8 +58,8 @@ template <bool TRACER> struct RpEuler {
         constexpr int mu = Dir<IXY>::MU, mv = Dir<IXY>::MV;
         const double gamma = prm[0], gamma1 = prm[1];
         // Roe averages, :87-104
-        const double rhsqrtl = sqrt(qL[0]);
-        const double rhsqrtr = sqrt(qR[0]);
+        const double rhsqrtl = dv.sqrt(qL[0]);
+        const double rhsqrtr = dv.sqrt(qR[0]);
         const double pl = gamma1 * (qL[3] - dv(0.5 * (qL[1] * qL[1] + qL[2] * qL[2]), qL[0]));
         const double pr = gamma1 * (qR[3] - dv(0.5 * (qR[1] * qR[1] + qR[2] * qR[2]), qR[0]));
         const double rhsq2 = rhsqrtl + rhsqrtr;
@@ -67,7 +68,7 @@ template <bool TRACER> struct RpEuler {
         const double enth = dv(dv(qL[3] + pl, rhsqrtl) + dv(qR[3] + pr, rhsqrtr), rhsq2);
         const double u2v2 = u * u + v * v;
         const double asq = gamma1 * (enth - .5 * u2v2);
-        const double a = sqrt(asq);
+        const double a = dv.sqrt(asq);
         const double g1a2 = dv(gamma1, asq);
         const double euv = enth - u2v2;
         roe[0] = u; roe[1] = v; roe[2] = a; roe[3] = enth; roe[4] = u2v2; roe[5] = g1a2; roe[6] = euv;
@@ -102,7 +103,7 @@ template <bool TRACER> struct RpEuler {
             // gamma1*(qr(4,i-1) - 0.5*(qr(mu,i-1)**2 + qr(mv,i-1)**2)/rhoim1) is pl bit for bit:
             // the two squares are the same and IEEE addition commutes
             const double pim1 = pl;
-            const double cim1 = sqrt(dv(gamma * pim1, rhoim1));
+            const double cim1 = dv.sqrt(dv(gamma * pim1, rhoim1));
             const double s0 = dv(qL[mu], rhoim1) - cim1;
             if (s0 >= 0.0 && s[0] > 0.0) {
 #pragma unroll
@@ -113,7 +114,7 @@ template <bool TRACER> struct RpEuler {
                 const double rhov1 = qL[mv] + wave[0][mv];
                 const double en1 = qL[3] + wave[0][3];
                 const double p1 = gamma1 * (en1 - dv(0.5 * (rhou1 * rhou1 + rhov1 * rhov1), rho1));
-                const double c1 = sqrt(dv(gamma * p1, rho1));
+                const double c1 = dv.sqrt(dv(gamma * p1, rho1));
                 const double s1 = dv(rhou1, rho1) - c1;
                 double sfract;
                 if (s0 < 0.0 && s1 > 0.0) sfract = dv(s0 * (s1 - s[0]), s1 - s0);
@@ -133,14 +134,14 @@ template <bool TRACER> struct RpEuler {
                     if constexpr (TRACER) amdq[4] = amdq[4] + s[4] * wave[4][4];
                     const double rhoi = qR[0];
                     const double pi = pr;   // same value as pr, see pim1
-                    const double ci = sqrt(dv(gamma * pi, rhoi));
+                    const double ci = dv.sqrt(dv(gamma * pi, rhoi));
                     const double s3 = dv(qR[mu], rhoi) + ci;
                     const double rho2 = qR[0] - wave[3][0];
                     const double rhou2 = qR[mu] - wave[3][mu];
                     const double rhov2 = qR[mv] - wave[3][mv];
                     const double en2 = qR[3] - wave[3][3];
                     const double p2 = gamma1 * (en2 - dv(0.5 * (rhou2 * rhou2 + rhov2 * rhov2), rho2));
-                    const double c2 = sqrt(dv(gamma * p2, rho2));
+                    const double c2 = dv.sqrt(dv(gamma * p2, rho2));
                     const double s2 = dv(rhou2, rho2) + c2;
                     bool add4 = true;
                     if (s2 < 0.0 && s3 > 0.0) sfract = dv(s2 * (s3 - s[3]), s3 - s2);
@@ -315,12 +316,12 @@ struct RpShallow {
         constexpr int mu = Dir<IXY>::MU, mv = Dir<IXY>::MV;
         const double grav = prm[0];
         const double hl = qL[0], hr = qR[0];
-        const double hsqrtl = sqrt(hl), hsqrtr = sqrt(hr);
+        const double hsqrtl = dv.sqrt(hl), hsqrtr = dv.sqrt(hr);
         const double hsq2 = hsqrtl + hsqrtr;
         const double ubar = dv(dv(qL[mu], hsqrtl) + dv(qR[mu], hsqrtr), hsq2);
         const double vbar = dv(dv(qL[mv], hsqrtl) + dv(qR[mv], hsqrtr), hsq2);
         const double hbar = 0.5 * (hl + hr);
-        const double cbar = sqrt(grav * hbar);
+        const double cbar = dv.sqrt(grav * hbar);
         const double delta1 = hr - hl;
         const double delta2 = qR[mu] - qL[mu];
         const double delta3 = qR[mv] - qL[mv];
@@ -332,13 +333,13 @@ struct RpShallow {
         wave[1][0] = 0.0; wave[1][mu] = 0.0; wave[1][mv] = a2; s[1] = ubar;
         wave[2][0] = a3; wave[2][mu] = a3 * (ubar + cbar); wave[2][mv] = a3 * vbar; s[2] = ubar + cbar;
 
-        const double s0 = dv(qL[mu], hl) - sqrt(grav * hl);
+        const double s0 = dv(qL[mu], hl) - dv.sqrt(grav * hl);
         if (s0 >= 0.0 && s[0] > 0.0) {
             amdq[0] = 0.0; amdq[1] = 0.0; amdq[2] = 0.0;
         } else {
             const double h1 = hl + wave[0][0];
             const double hu1 = qL[mu] + wave[0][mu];
-            const double s1 = dv(hu1, h1) - sqrt(grav * h1);
+            const double s1 = dv(hu1, h1) - dv.sqrt(grav * h1);
             double sfract;
             if (s0 < 0.0 && s1 > 0.0) sfract = dv(s0 * (s1 - s[0]), s1 - s0);
             else if (s[0] < 0.0) sfract = s[0];
@@ -347,10 +348,10 @@ struct RpShallow {
             for (int m = 0; m < MEQN; m++) amdq[m] = sfract * wave[0][m];
             if (s[1] < 0.0) {
                 amdq[mv] = amdq[mv] + s[1] * wave[1][mv];
-                const double s3 = dv(qR[mu], hr) + sqrt(grav * hr);
+                const double s3 = dv(qR[mu], hr) + dv.sqrt(grav * hr);
                 const double h2 = hr - wave[2][0];
                 const double hu2 = qR[mu] - wave[2][mu];
-                const double s2 = dv(hu2, h2) + sqrt(grav * h2);
+                const double s2 = dv(hu2, h2) + dv.sqrt(grav * h2);
                 bool add3 = true;
                 if (s2 < 0.0 && s3 > 0.0) sfract = dv(s2 * (s3 - s[2]), s3 - s2);
                 else if (s[2] < 0.0) sfract = s[2];

@@ -1,15 +1,16 @@
-"""The branch-free division of the Riemann solvers and the limiter.
+"""The branch-free division and square root of the Riemann solvers and the
+limiter.
 
-The kernels divide with FastDiv (pyclaw_b200/csrc/claw2_fastdiv.cuh): a
-Newton-Raphson quotient plus a proof, from the exact FMA remainder, that the
-quotient is the correctly rounded one; a solve whose proofs did not all pass
-is redone with IEEE division.  These tests call the division on the GPU
-through claw2_fastdiv_check and require, over many millions of operand pairs
-(random over the whole exponent range, typical solver magnitudes and the hard
-cases of division), that every quotient it marks as proven equals the IEEE
-quotient bit for bit (numpy's division on the host), that the proof fails for
-every operand outside its range, and that it passes for nearly all operands of
-ordinary size.
+The kernels divide and take square roots with FastRn
+(pyclaw_b200/csrc/claw2_fastrn.cuh): a Newton-Raphson result plus a proof,
+from the exact FMA remainder, that it is the correctly rounded one; a tile
+whose proofs did not all pass is redone with IEEE arithmetic.  These tests call
+both operations on the GPU through claw2_fastrn_check and require, over many
+millions of operands (random over the whole exponent range, typical solver
+magnitudes and the hard cases), that every result marked as proven equals the
+IEEE result bit for bit (numpy's division and square root on the host), that
+the proof fails for every operand outside its range, and that it passes for
+nearly all operands of ordinary size.
 """
 import ctypes
 
@@ -22,19 +23,28 @@ from pyclaw_b200 import _lib
 pytestmark = pytest.mark.gpu
 
 
-def _fastdiv(a, b):
+def _fastrn(op, a, b=None):
     t = H.torch()
     lib = _lib.load()
     da = t.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).cuda()
-    db = t.from_numpy(np.ascontiguousarray(b, dtype=np.float64)).cuda()
+    db = t.from_numpy(np.ascontiguousarray(b, dtype=np.float64)).cuda() if b is not None else None
     q = t.empty_like(da)
     ok = t.empty(da.shape, dtype=t.uint8, device='cuda')
-    rc = lib.claw2_fastdiv_check(ctypes.c_void_p(da.data_ptr()), ctypes.c_void_p(db.data_ptr()),
-                                 ctypes.c_void_p(q.data_ptr()), ctypes.c_void_p(ok.data_ptr()), da.numel(),
-                                 H.stream())
+    rc = lib.claw2_fastrn_check(op, ctypes.c_void_p(da.data_ptr()),
+                                ctypes.c_void_p(db.data_ptr()) if db is not None else None,
+                                ctypes.c_void_p(q.data_ptr()), ctypes.c_void_p(ok.data_ptr()), da.numel(),
+                                H.stream())
     assert rc == 0, _lib.load().claw2_strerror(rc)
     t.cuda.synchronize()
     return q.cpu().numpy(), ok.cpu().numpy().astype(bool)
+
+
+def _fastdiv(a, b):
+    return _fastrn(0, a, b)
+
+
+def _fastsqrt(x):
+    return _fastrn(1, x)
 
 
 def _bits(x):
@@ -140,3 +150,63 @@ def test_zeros_signs_and_out_of_range_operands():
     # never proven: quotients out of range, infinite or NaN dividends
     _, oo = _fastdiv(np.array([1e-150, 1e150, np.inf, np.nan]), np.array([1e100, 1e-100, 1.0, 1.0]))
     assert not oo.any()
+
+
+def _check_sqrt(x):
+    """Every proven root equals numpy's IEEE root bit for bit.  Returns the
+    proven fraction and mask."""
+    r, ok = _fastsqrt(x)
+    with np.errstate(all='ignore'):
+        ref = np.sqrt(x)
+    bad = ok & (_bits(r) != _bits(ref))
+    assert not bad.any(), (x[bad][:5], r[bad][:5], ref[bad][:5])
+    return ok.mean(), ok
+
+
+def test_sqrt_random_and_ordinary():
+    rng = np.random.default_rng(31)
+    n = 1 << 23
+    for _ in range(3):
+        _check_sqrt(np.abs(_random_doubles(rng, n, -1022, 1023)))
+        _check_sqrt(_random_doubles(rng, n, -1022, 1023))           # half negative: never proven
+    for lo, hi in ((1e-3, 1e3), (1e-12, 1e-6), (1e6, 1e12)):
+        frac, _ = _check_sqrt(rng.uniform(lo, hi, n))
+        assert frac > 1.0 - 1e-6, frac
+    frac, _ = _check_sqrt(np.abs(_random_doubles(rng, n, -900, 1000)))
+    assert frac > 1.0 - 1e-6, frac
+
+
+def test_sqrt_hard_cases():
+    """Perfect squares (exact roots), squares of doubles and their neighbours
+    (roots next to a midpoint), arguments next to powers of four (roots next
+    to a power of two) and all-ones significands."""
+    rng = np.random.default_rng(37)
+    n = 1 << 22
+    m = rng.integers(1, 1 << 26, n).astype(np.float64)
+    scale = np.ldexp(1.0, 2 * rng.integers(-200, 200, n))
+    frac, _ = _check_sqrt(m * m * scale)
+    assert frac == 1.0
+    s = np.abs(_random_doubles(rng, n, -300, 300))
+    sq = s * s
+    for x in (sq, np.nextafter(sq, np.inf), np.nextafter(sq, 0.0)):
+        frac, _ = _check_sqrt(x)
+        assert frac > 1.0 - 1e-6, frac
+    k = rng.integers(0, 64, n, dtype=np.uint64)
+    exp = rng.integers(1023 - 300, 1023 + 300, n).astype(np.uint64) << np.uint64(52)
+    ones = np.uint64((1 << 52) - 1)
+    for x in ((exp | k).view(np.float64), (exp | (ones - k)).view(np.float64)):
+        frac, _ = _check_sqrt(x)
+        assert frac > 0.9, frac      # roots next to a power of two use the smaller gap
+
+
+def test_sqrt_specials_are_never_proven():
+    tiny = np.nextafter(0.0, 1.0)
+    x = np.array([0.0, -0.0, -1.0, -1e-300, tiny, 2.2250738585072014e-308, 2.0 ** -961, np.inf, -np.inf, np.nan])
+    r, ok = _fastsqrt(x)
+    assert not ok.any(), x[ok]
+    x = np.array([2.0 ** -960, 1.0, 4.0, 2.0, 0.25])
+    r, ok = _fastsqrt(x)
+    assert ok.all()
+    assert (_bits(r) == _bits(np.sqrt(x))).all()
+    # the largest double: its root lies next to a midpoint below 2^512
+    _check_sqrt(np.array([np.finfo(np.float64).max, np.nextafter(2.0 ** 1022, 0.0)]))
