@@ -193,15 +193,6 @@ CLAW2_EXPORT int claw2_step(const claw2_problem* p, const double* q_in, double* 
 CLAW2_EXPORT int claw2_step_noalloc(const claw2_problem* p, const double* q_in, double* q_out,
                                     const double* aux, double dt, double* cfl_dev, void* stream);
 
-/* Self-check of the branch-free division and square root used by the Riemann
- * solvers and the limiter (no counterpart in the reference, whose Fortran uses
- * the CPU's IEEE operations).  For k < n (device arrays): out[k] = the fast
- * a[k]/b[k] (op 0) or sqrt(a[k]) (op 1, b unused and may be NULL), ok[k] = 1
- * when the kernel proved out[k] to be the correctly rounded result, 0 when a
- * solve would redo it with IEEE arithmetic. */
-CLAW2_EXPORT int claw2_fastrn_check(int op, const double* a, const double* b, double* out, unsigned char* ok,
-                                    int64_t n, void* stream);
-
 /* Launch nsteps controlled steps.  q0/q1 are the two state buffers; ctrl->cur
  * says which holds the current state.  Each launch reads dt from ctrl, steps
  * q[cur] -> q[1-cur] and updates ctrl exactly as one iteration of

@@ -22,7 +22,6 @@ SRCS = [os.path.join(HERE, "csrc", "claw2_capi.cu"),
 OBJDIR = os.path.join(HERE, "_build")
 DEPS = SRCS + [os.path.join(HERE, "csrc", "claw2_kernels.cuh"),
                os.path.join(HERE, "csrc", "claw2_riemann.cuh"),
-               os.path.join(HERE, "csrc", "claw2_fastrn.cuh"),
                os.path.join(HERE, "csrc", "claw2_light.cuh"),
                os.path.join(ROOT, "include", "claw2.h"),
                os.path.join(ROOT, "include", "claw2_adjoint.h")]

@@ -155,20 +155,6 @@ __global__ void fill_kernel_ctrl(FillArgs f, double* q0, double* q1, const claw2
 
 // ---------------------------------------------------------------------------
 // layout conversion: reference (m fastest, Fortran) <-> device (planes)
-
-// The branch-free division and square root of the Riemann solvers on
-// arbitrary operands: out[k] = FastRn a[k]/b[k] (op 0) or sqrt(a[k]) (op 1),
-// ok[k] = whether it proved out[k] correctly rounded.
-__global__ void fastrn_kernel(int op, const double* __restrict__ a, const double* __restrict__ b,
-                              double* __restrict__ out, unsigned char* __restrict__ ok, int64_t n)
-{
-    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
-        claw2::FastRn f;
-        out[k] = op == 0 ? f(a[k], b[k]) : f.sqrt(a[k]);
-        ok[k] = f.ok ? 1 : 0;
-    }
-}
-
 // ---------------------------------------------------------------------------
 __global__ void ref_to_dev_kernel(const double* ref, double* dev, int nc, int nx, int ny, long long ld,
                                   long long plane, int ghosts_in_ref)
@@ -627,17 +613,6 @@ int claw2_device_to_ref(const claw2_problem* p, int ncomp, const double* dev, do
 {
     if (!p || !ref || !dev || ncomp < 1) return CLAW2_ERR_INVALID;
     return conv(p, ncomp, dev, ref, false, true, S(stream));
-}
-
-int claw2_fastrn_check(int op, const double* a, const double* b, double* out, unsigned char* ok, int64_t n,
-                       void* stream)
-{
-    if (op != 0 && op != 1) return CLAW2_ERR_INVALID;
-    if (n < 0 || (n > 0 && (!a || (op == 0 && !b) || !out || !ok))) return CLAW2_ERR_INVALID;
-    if (n == 0) return CLAW2_OK;
-    const int64_t blocks = (n + 255) / 256;
-    fastrn_kernel<<<(unsigned)(blocks < 148 * 64 ? blocks : 148 * 64), 256, 0, S(stream)>>>(op, a, b, out, ok, n);
-    return cudaGetLastError() == cudaSuccess ? CLAW2_OK : CLAW2_ERR_CUDA;
 }
 
 // ---------------------------------------------------------------------------

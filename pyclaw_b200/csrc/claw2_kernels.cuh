@@ -66,10 +66,10 @@ CLAW2_HD long long qoff(const StepArgs& a, int m, int i, int j)
     return (long long)m * a.plane + (long long)(j + CLAW2_NUM_GHOST) * a.ld + (i + CLAW2_NUM_GHOST);
 }
 
-// philim.f90:18-55 as a function of r = b/a; ids outside 1..5 fall through to
-// minmod like the computed GOTO
-CLAW2_HD double philim_r(double r, int meth)
+// philim.f90:18-55; ids outside 1..5 fall through to minmod like the computed GOTO
+CLAW2_HD double philim(double a, double b, int meth)
 {
+    const double r = b / a;
     double t, u;
     switch (meth) {
     case 2:
@@ -91,19 +91,6 @@ CLAW2_HD double philim_r(double r, int meth)
         t = 1.0 < r ? 1.0 : r;
         return 0.0 > t ? 0.0 : t;
     }
-}
-
-// philim(wnorm2, dot, meth) with r = dot/wnorm2 divided by the policy dv
-template <class DV>
-CLAW2_HD double philim(double a, double b, int meth, DV& dv)
-{
-    return philim_r(dv(b, a), meth);
-}
-
-CLAW2_HD double philim(double a, double b, int meth)
-{
-    IeeeRn d;
-    return philim(a, b, meth, d);
 }
 
 // One iteration of Solver.evolve_to_time after the step (src/pyclaw/solver.py:650-691)
@@ -234,10 +221,10 @@ template <class RP, int TX, int TY, int NT, bool SPLIT> struct TileSmem {
 // SPLIT = dimensional splitting (no transverse terms; each cell gets exactly
 // one contribution per sweep, so S4 is skipped).
 // ---------------------------------------------------------------------------
-template <class RP, int IXY, bool SPLIT, int TX, int TY, int NT, class Ctx, class DV>
+template <class RP, int IXY, bool SPLIT, int TX, int TY, int NT, class Ctx>
 CLAW2_HD void sweep_chunk(const StepArgs& a, Ctx& ctx, const double* qin, double* Qx, double* WB, double* B2,
                           int i0, int j0, int line, int cfirst, int clast, bool lineok, bool cflonly,
-                          double dtn, double dtt, double& cflm, DV& dv)
+                          double dtn, double dtt, double& cflm)
 {
     constexpr int MEQN = RP::MEQN, MW = RP::MW, MAUX = RP::MAUX, NROE = RP::NROE;
     constexpr int QROWS = SPLIT ? TY + 4 : TY;
@@ -288,7 +275,7 @@ CLAW2_HD void sweep_chunk(const StepArgs& a, Ctx& ctx, const double* qin, double
             auxL[m] = a.aux[oL + m * a.plane];
             auxR[m] = a.aux[oR + m * a.plane];
         }
-        RP::template rpn2<IXY>(qL, qR, auxL, auxR, a.prm, wave, s, amdq, apdq, roe, dv);
+        RP::template rpn2<IXY>(qL, qR, auxL, auxR, a.prm, wave, s, amdq, apdq, roe);
 #pragma unroll
         for (int p = 0; p < MW; p++) {
 #pragma unroll
@@ -343,7 +330,7 @@ CLAW2_HD void sweep_chunk(const StepArgs& a, Ctx& ctx, const double* qin, double
                         double dot = 0.0;
 #pragma unroll
                         for (int m = 0; m < MEQN; m++) dot = dot + wv[m] * W(p, m, nb);
-                        const double phi = philim(wnorm2, dot, meth, dv);
+                        const double phi = philim(wnorm2, dot, meth);
 #pragma unroll
                         for (int m = 0; m < MEQN; m++) wv[m] = phi * wv[m];
                     }
@@ -383,7 +370,7 @@ CLAW2_HD void sweep_chunk(const StepArgs& a, Ctx& ctx, const double* qin, double
                     ax2[m] = a.aux[o1 + m * a.plane];
                     ax3[m] = a.aux[o1 + across + m * a.plane];
                 }
-                RP::template rpt2<IXY>(1, A, roe, ax1, ax2, ax3, a.prm, bmL, bpL, dv);
+                RP::template rpt2<IXY>(1, A, roe, ax1, ax2, ax3, a.prm, bmL, bpL);
             }
             {
                 const long long o2 = o1 + along;
@@ -393,7 +380,7 @@ CLAW2_HD void sweep_chunk(const StepArgs& a, Ctx& ctx, const double* qin, double
                     ax2[m] = a.aux[o2 + m * a.plane];
                     ax3[m] = a.aux[o2 + across + m * a.plane];
                 }
-                RP::template rpt2<IXY>(2, P, roe, ax1, ax2, ax3, a.prm, bmR, bpR, dv);
+                RP::template rpt2<IXY>(2, P, roe, ax1, ax2, ax3, a.prm, bmR, bpR);
             }
         }
         // publish what the cell left of the interface needs (own slot only)
@@ -619,14 +606,36 @@ CLAW2_HD void finish_tile(const StepArgs& a, Ctx& ctx, const TileId& tile, const
     }
 }
 
-// The x sweeps then the y sweeps of one tile, LPC = NT/32 lines per chunk,
-// ending with a block barrier; Qx then holds the tile's updated cells.
-template <class RP, int TX, int TY, int NT, bool SPLIT, class Ctx, class DV>
-CLAW2_HD void tile_sweeps(const StepArgs& a, Ctx& ctx, const double* qin, double* Qx, double* WB, double* B2,
-                          int i0, int j0, double dtdx, double dtdy, double& cflm, DV& dv)
+template <class RP, int TX, int TY, int NT, bool SPLIT, class Ctx>
+CLAW2_HD void step_tile_at(const StepArgs& a, Ctx& ctx, const TileId& tile)
 {
+    constexpr int MEQN = RP::MEQN;
     constexpr int LPC = NT / 32;
-    const int warp = ctx.tid() >> 5;
+    static_assert(NT % 32 == 0, "NT must be a multiple of 32");
+    static_assert(TX + 3 <= 32 && TY + 3 <= 32, "tile too wide for one 32-lane line");
+    using SM = TileSmem<RP, TX, TY, NT, SPLIT>;
+    constexpr int QROWS = SM::QROWS;
+    constexpr int QROW0 = SPLIT ? -2 : 0;
+    double* Qx = ctx.smem();
+    double* WB = Qx + SM::QX;
+    double* B2 = WB + SM::WBSZ * NT;
+    double* red = B2 + SM::B2SZ * NT;
+    const int tid = ctx.tid();
+    const int warp = tid >> 5;
+    const int i0 = tile.bx * TX, j0 = tile.by * TY;
+
+    const double* qin = a.qin;
+    double* qout = a.qout;
+    double dt = a.dt;
+    if (a.ctrl) {
+        if (a.ctrl->done) return;                  // uniform across the grid
+        dt = a.ctrl->dt;
+        const int cur = a.ctrl->cur;
+        qin = cur ? a.q1 : a.q0;
+        qout = cur ? a.q0 : a.q1;
+    }
+    const double dtdx = dt / a.dx, dtdy = dt / a.dy;
+    double cflm = 0.0;
 
     // ---- x sweeps: unsplit slices j0-1..j0+TY (rows -1..my); split rows j0-2..j0+TY+1
     {
@@ -638,7 +647,7 @@ CLAW2_HD void tile_sweeps(const StepArgs& a, Ctx& ctx, const double* qin, double
             const int line = c0 + warp;
             const int clast = (c0 + LPC - 1 < last) ? c0 + LPC - 1 : last;
             sweep_chunk<RP, 1, SPLIT, TX, TY, NT>(a, ctx, qin, Qx, WB, B2, i0, j0, line, c0, clast,
-                                                  line <= last, false, dtdx, dtdy, cflm, dv);
+                                                  line <= last, false, dtdx, dtdy, cflm);
             if (SPLIT) ctx.sync();
         }
     }
@@ -654,7 +663,7 @@ CLAW2_HD void tile_sweeps(const StepArgs& a, Ctx& ctx, const double* qin, double
                 const int line = c0 + warp;
                 const int clast = (c0 + LPC - 1 < last) ? c0 + LPC - 1 : last;
                 sweep_chunk<RP, 2, SPLIT, TX, TY, NT>(a, ctx, qin, Qx, WB, B2, i0, j0, line, c0, clast,
-                                                      line <= last, false, dtdy, dtdx, cflm, dv);
+                                                      line <= last, false, dtdy, dtdx, cflm);
             }
         } else {
             const int nlines = ninner + (left ? 2 : 0) + (right ? 2 : 0);
@@ -669,54 +678,12 @@ CLAW2_HD void tile_sweeps(const StepArgs& a, Ctx& ctx, const double* qin, double
                     else { line = a.mx + (r - ninner); cflonly = true; }
                 }
                 sweep_chunk<RP, 2, SPLIT, TX, TY, NT>(a, ctx, qin, Qx, WB, B2, i0, j0, line, 0, 0,
-                                                      l < nlines, cflonly, dtdy, dtdx, cflm, dv);
+                                                      l < nlines, cflonly, dtdy, dtdx, cflm);
                 ctx.sync();
             }
         }
     }
-}
 
-template <class RP, int TX, int TY, int NT, bool SPLIT, class Ctx>
-CLAW2_HD void step_tile_at(const StepArgs& a, Ctx& ctx, const TileId& tile)
-{
-    constexpr int MEQN = RP::MEQN;
-    static_assert(NT % 32 == 0, "NT must be a multiple of 32");
-    static_assert(TX + 3 <= 32 && TY + 3 <= 32, "tile too wide for one 32-lane line");
-    using SM = TileSmem<RP, TX, TY, NT, SPLIT>;
-    constexpr int QROWS = SM::QROWS;
-    constexpr int QROW0 = SPLIT ? -2 : 0;
-    double* Qx = ctx.smem();
-    double* WB = Qx + SM::QX;
-    double* B2 = WB + SM::WBSZ * NT;
-    double* red = B2 + SM::B2SZ * NT;
-    const int i0 = tile.bx * TX, j0 = tile.by * TY;
-
-    const double* qin = a.qin;
-    double* qout = a.qout;
-    double dt = a.dt;
-    if (a.ctrl) {
-        if (a.ctrl->done) return;                  // uniform across the grid
-        dt = a.ctrl->dt;
-        const int cur = a.ctrl->cur;
-        qin = cur ? a.q1 : a.q0;
-        qout = cur ? a.q0 : a.q1;
-    }
-    const double dtdx = dt / a.dx, dtdy = dt / a.dy;
-    double cflm = 0.0;
-#if defined(__CUDA_ARCH__)
-    // The sweeps rebuild Qx from qin alone, so a tile can be redone: with
-    // IEEE division when a FastRn quotient was not proven correctly rounded.
-    FastRn f;
-    tile_sweeps<RP, TX, TY, NT, SPLIT>(a, ctx, qin, Qx, WB, B2, i0, j0, dtdx, dtdy, cflm, f);
-    if (__syncthreads_or(!f.ok)) {
-        IeeeRn d;
-        cflm = 0.0;
-        tile_sweeps<RP, TX, TY, NT, SPLIT>(a, ctx, qin, Qx, WB, B2, i0, j0, dtdx, dtdy, cflm, d);
-    }
-#else
-    IeeeRn d;
-    tile_sweeps<RP, TX, TY, NT, SPLIT>(a, ctx, qin, Qx, WB, B2, i0, j0, dtdx, dtdy, cflm, d);
-#endif
     finish_tile<MEQN, TX, TY, NT>(a, ctx, tile, Qx + (-QROW0) * TX, QROWS * TX, red, qout, i0, j0, cflm, dt);
 }
 

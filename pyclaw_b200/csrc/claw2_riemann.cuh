@@ -12,12 +12,6 @@
 // --fmad=false), so results agree bit for bit with the CPU oracle except for
 // the sign of exact zeros where a structurally zero term is skipped.
 //
-// Divisions and square roots go through the policy object dv
-// (claw2_fastrn.cuh): dv(a, b) = a/b, dv.sqrt(x).  FastRn computes the
-// correctly rounded result without a slow-path branch, or flags that it could
-// not prove it; the tile kernel then redoes the tile with IeeeRn, so every
-// result is the IEEE one.
-//
 // Indexing: qL is the cell left of the interface (Fortran qr(:,i-1)), qR the
 // cell right of it (Fortran ql(:,i)).  IXY = 1 for x slices, 2 for y slices;
 // MU/MV are the 0-based normal / transverse momentum components.
@@ -25,7 +19,6 @@
 
 #if defined(__CUDACC__)
 #define CLAW2_DEV __device__ __forceinline__
-#include "claw2_fastrn.cuh"
 #else
 #include <cmath>
 #define CLAW2_DEV inline
@@ -49,27 +42,28 @@ template <bool TRACER> struct RpEuler {
     static constexpr int MAUX = 0;
     static constexpr int NROE = 7;   // u, v, a, enth, u2v2, g1a2, euv
 
-    template <int IXY, class DV>
+    template <int IXY>
     static CLAW2_DEV void rpn2(const double (&qL)[MEQN], const double (&qR)[MEQN],
-                               const double*, const double*, const double* prm,
-                               double (&wave)[MW][MEQN], double (&s)[MW],
-                               double (&amdq)[MEQN], double (&apdq)[MEQN], double (&roe)[NROE], DV& dv)
+                                                const double*, const double*, const double* prm,
+                                                double (&wave)[MW][MEQN], double (&s)[MW],
+                                                double (&amdq)[MEQN], double (&apdq)[MEQN],
+                                                double (&roe)[NROE])
     {
         constexpr int mu = Dir<IXY>::MU, mv = Dir<IXY>::MV;
         const double gamma = prm[0], gamma1 = prm[1];
         // Roe averages, :87-104
-        const double rhsqrtl = dv.sqrt(qL[0]);
-        const double rhsqrtr = dv.sqrt(qR[0]);
-        const double pl = gamma1 * (qL[3] - dv(0.5 * (qL[1] * qL[1] + qL[2] * qL[2]), qL[0]));
-        const double pr = gamma1 * (qR[3] - dv(0.5 * (qR[1] * qR[1] + qR[2] * qR[2]), qR[0]));
+        const double rhsqrtl = sqrt(qL[0]);
+        const double rhsqrtr = sqrt(qR[0]);
+        const double pl = gamma1 * (qL[3] - 0.5 * (qL[1] * qL[1] + qL[2] * qL[2]) / qL[0]);
+        const double pr = gamma1 * (qR[3] - 0.5 * (qR[1] * qR[1] + qR[2] * qR[2]) / qR[0]);
         const double rhsq2 = rhsqrtl + rhsqrtr;
-        const double u = dv(dv(qL[mu], rhsqrtl) + dv(qR[mu], rhsqrtr), rhsq2);
-        const double v = dv(dv(qL[mv], rhsqrtl) + dv(qR[mv], rhsqrtr), rhsq2);
-        const double enth = dv(dv(qL[3] + pl, rhsqrtl) + dv(qR[3] + pr, rhsqrtr), rhsq2);
+        const double u = (qL[mu] / rhsqrtl + qR[mu] / rhsqrtr) / rhsq2;
+        const double v = (qL[mv] / rhsqrtl + qR[mv] / rhsqrtr) / rhsq2;
+        const double enth = ((qL[3] + pl) / rhsqrtl + (qR[3] + pr) / rhsqrtr) / rhsq2;
         const double u2v2 = u * u + v * v;
         const double asq = gamma1 * (enth - .5 * u2v2);
-        const double a = dv.sqrt(asq);
-        const double g1a2 = dv(gamma1, asq);
+        const double a = sqrt(asq);
+        const double g1a2 = gamma1 / asq;
         const double euv = enth - u2v2;
         roe[0] = u; roe[1] = v; roe[2] = a; roe[3] = enth; roe[4] = u2v2; roe[5] = g1a2; roe[6] = euv;
 
@@ -80,7 +74,7 @@ template <bool TRACER> struct RpEuler {
         const double d3 = qR[3] - qL[3];
         const double a3 = g1a2 * (euv * d0 + u * d1 + v * d2 - d3);
         const double a2 = d2 - v * d0;
-        const double a4 = dv(d1 + (a - u) * d0 - a * a3, 2.0 * a);
+        const double a4 = (d1 + (a - u) * d0 - a * a3) / (2.0 * a);
         const double a1 = d0 - a3 - a4;
         wave[0][0] = a1; wave[0][mu] = a1 * (u - a); wave[0][mv] = a1 * v; wave[0][3] = a1 * (enth - u * a);
         s[0] = u - a;
@@ -103,8 +97,8 @@ template <bool TRACER> struct RpEuler {
             // gamma1*(qr(4,i-1) - 0.5*(qr(mu,i-1)**2 + qr(mv,i-1)**2)/rhoim1) is pl bit for bit:
             // the two squares are the same and IEEE addition commutes
             const double pim1 = pl;
-            const double cim1 = dv.sqrt(dv(gamma * pim1, rhoim1));
-            const double s0 = dv(qL[mu], rhoim1) - cim1;
+            const double cim1 = sqrt(gamma * pim1 / rhoim1);
+            const double s0 = qL[mu] / rhoim1 - cim1;
             if (s0 >= 0.0 && s[0] > 0.0) {
 #pragma unroll
                 for (int m = 0; m < MEQN; m++) amdq[m] = 0.0;
@@ -113,11 +107,11 @@ template <bool TRACER> struct RpEuler {
                 const double rhou1 = qL[mu] + wave[0][mu];
                 const double rhov1 = qL[mv] + wave[0][mv];
                 const double en1 = qL[3] + wave[0][3];
-                const double p1 = gamma1 * (en1 - dv(0.5 * (rhou1 * rhou1 + rhov1 * rhov1), rho1));
-                const double c1 = dv.sqrt(dv(gamma * p1, rho1));
-                const double s1 = dv(rhou1, rho1) - c1;
+                const double p1 = gamma1 * (en1 - 0.5 * (rhou1 * rhou1 + rhov1 * rhov1) / rho1);
+                const double c1 = sqrt(gamma * p1 / rho1);
+                const double s1 = rhou1 / rho1 - c1;
                 double sfract;
-                if (s0 < 0.0 && s1 > 0.0) sfract = dv(s0 * (s1 - s[0]), s1 - s0);
+                if (s0 < 0.0 && s1 > 0.0) sfract = s0 * (s1 - s[0]) / (s1 - s0);
                 else if (s[0] < 0.0) sfract = s[0];
                 else sfract = 0.0;
 #pragma unroll
@@ -134,17 +128,17 @@ template <bool TRACER> struct RpEuler {
                     if constexpr (TRACER) amdq[4] = amdq[4] + s[4] * wave[4][4];
                     const double rhoi = qR[0];
                     const double pi = pr;   // same value as pr, see pim1
-                    const double ci = dv.sqrt(dv(gamma * pi, rhoi));
-                    const double s3 = dv(qR[mu], rhoi) + ci;
+                    const double ci = sqrt(gamma * pi / rhoi);
+                    const double s3 = qR[mu] / rhoi + ci;
                     const double rho2 = qR[0] - wave[3][0];
                     const double rhou2 = qR[mu] - wave[3][mu];
                     const double rhov2 = qR[mv] - wave[3][mv];
                     const double en2 = qR[3] - wave[3][3];
-                    const double p2 = gamma1 * (en2 - dv(0.5 * (rhou2 * rhou2 + rhov2 * rhov2), rho2));
-                    const double c2 = dv.sqrt(dv(gamma * p2, rho2));
-                    const double s2 = dv(rhou2, rho2) + c2;
+                    const double p2 = gamma1 * (en2 - 0.5 * (rhou2 * rhou2 + rhov2 * rhov2) / rho2);
+                    const double c2 = sqrt(gamma * p2 / rho2);
+                    const double s2 = rhou2 / rho2 + c2;
                     bool add4 = true;
-                    if (s2 < 0.0 && s3 > 0.0) sfract = dv(s2 * (s3 - s[3]), s3 - s2);
+                    if (s2 < 0.0 && s3 > 0.0) sfract = s2 * (s3 - s[3]) / (s3 - s2);
                     else if (s[3] < 0.0) sfract = s[3];
                     else add4 = false;
                     if (add4) {
@@ -179,16 +173,16 @@ template <bool TRACER> struct RpEuler {
     }
 
     // rpt2_euler_5wave.f:47-95.  The split uses this interface's Roe averages.
-    template <int IXY, class DV>
+    template <int IXY>
     static CLAW2_DEV void rpt2(int, const double (&asdq)[MEQN], const double (&roe)[NROE],
-                               const double*, const double*, const double*,
-                               const double*, double (&bm)[MEQN], double (&bp)[MEQN], DV& dv)
+                                                const double*, const double*, const double*,
+                                                const double*, double (&bm)[MEQN], double (&bp)[MEQN])
     {
         constexpr int mu = Dir<IXY>::MU, mv = Dir<IXY>::MV;
         const double u = roe[0], v = roe[1], a = roe[2], enth = roe[3], u2v2 = roe[4], g1a2 = roe[5], euv = roe[6];
         const double a3 = g1a2 * (euv * asdq[0] + u * asdq[mu] + v * asdq[mv] - asdq[3]);
         const double a2 = asdq[mu] - u * asdq[0];
-        const double a4 = dv(asdq[mv] + (a - v) * asdq[0] - a * a3, 2.0 * a);
+        const double a4 = (asdq[mv] + (a - v) * asdq[0] - a * a3) / (2.0 * a);
         const double a1 = asdq[0] - a3 - a4;
         double wb[3][4];
         wb[0][0] = a1; wb[0][mu] = a1 * u; wb[0][mv] = a1 * (v - a); wb[0][3] = a1 * (enth - v * a);
@@ -221,34 +215,34 @@ template <bool TRACER> struct RpEuler {
 struct RpAcoustics {
     static constexpr int MEQN = 3, MW = 2, MAUX = 0, NROE = 1;
 
-    template <int IXY, class DV>
+    template <int IXY>
     static CLAW2_DEV void rpn2(const double (&qL)[MEQN], const double (&qR)[MEQN],
                                                 const double*, const double*, const double* prm,
                                                 double (&wave)[MW][MEQN], double (&s)[MW],
                                                 double (&amdq)[MEQN], double (&apdq)[MEQN],
-                                                double (&)[NROE], DV& dv)
+                                                double (&)[NROE])
     {
         constexpr int mu = Dir<IXY>::MU, mv = Dir<IXY>::MV;
         const double cc = prm[2], zz = prm[3];
         const double delta1 = qR[0] - qL[0];
         const double delta2 = qR[mu] - qL[mu];
-        const double a1 = dv(-delta1 + zz * delta2, 2.0 * zz);
-        const double a2 = dv(delta1 + zz * delta2, 2.0 * zz);
+        const double a1 = (-delta1 + zz * delta2) / (2.0 * zz);
+        const double a2 = (delta1 + zz * delta2) / (2.0 * zz);
         wave[0][0] = -a1 * zz; wave[0][mu] = a1; wave[0][mv] = 0.0; s[0] = -cc;
         wave[1][0] = a2 * zz;  wave[1][mu] = a2; wave[1][mv] = 0.0; s[1] = cc;
         amdq[0] = s[0] * wave[0][0]; amdq[mu] = s[0] * wave[0][mu]; amdq[mv] = 0.0;
         apdq[0] = s[1] * wave[1][0]; apdq[mu] = s[1] * wave[1][mu]; apdq[mv] = 0.0;
     }
 
-    template <int IXY, class DV>
+    template <int IXY>
     static CLAW2_DEV void rpt2(int, const double (&asdq)[MEQN], const double (&)[NROE],
                                                 const double*, const double*, const double*,
-                                                const double* prm, double (&bm)[MEQN], double (&bp)[MEQN], DV& dv)
+                                                const double* prm, double (&bm)[MEQN], double (&bp)[MEQN])
     {
         constexpr int mu = Dir<IXY>::MU, mv = Dir<IXY>::MV;
         const double cc = prm[2], zz = prm[3];
-        const double a1 = dv(-asdq[0] + zz * asdq[mv], 2.0 * zz);
-        const double a2 = dv(asdq[0] + zz * asdq[mv], 2.0 * zz);
+        const double a1 = (-asdq[0] + zz * asdq[mv]) / (2.0 * zz);
+        const double a2 = (asdq[0] + zz * asdq[mv]) / (2.0 * zz);
         bm[0] = cc * a1 * zz; bm[mu] = 0.0; bm[mv] = -cc * a1;
         bp[0] = cc * a2 * zz; bp[mu] = 0.0; bp[mv] = cc * a2;
     }
@@ -262,20 +256,20 @@ struct RpAcoustics {
 struct RpVcAcoustics {
     static constexpr int MEQN = 3, MW = 2, MAUX = 2, NROE = 1;
 
-    template <int IXY, class DV>
+    template <int IXY>
     static CLAW2_DEV void rpn2(const double (&qL)[MEQN], const double (&qR)[MEQN],
                                                 const double* auxL, const double* auxR, const double*,
                                                 double (&wave)[MW][MEQN], double (&s)[MW],
                                                 double (&amdq)[MEQN], double (&apdq)[MEQN],
-                                                double (&)[NROE], DV& dv)
+                                                double (&)[NROE])
     {
         constexpr int mu = Dir<IXY>::MU, mv = Dir<IXY>::MV;
         const double zi = auxR[0] * auxR[1];
         const double zim = auxL[0] * auxL[1];
         const double delta1 = qR[0] - qL[0];
         const double delta2 = qR[mu] - qL[mu];
-        const double a1 = dv(-delta1 + zi * delta2, zim + zi);
-        const double a2 = dv(delta1 + zim * delta2, zim + zi);
+        const double a1 = (-delta1 + zi * delta2) / (zim + zi);
+        const double a2 = (delta1 + zim * delta2) / (zim + zi);
         wave[0][0] = -a1 * zim; wave[0][mu] = a1; wave[0][mv] = 0.0; s[0] = -auxL[1];
         wave[1][0] = a2 * zi;   wave[1][mu] = a2; wave[1][mv] = 0.0; s[1] = auxR[1];
         amdq[0] = s[0] * wave[0][0]; amdq[mu] = s[0] * wave[0][mu]; amdq[mv] = 0.0;
@@ -283,18 +277,18 @@ struct RpVcAcoustics {
     }
 
     // a1/a2/a3: aux of cell i1 in the slice below, in the slice, and above.
-    template <int IXY, class DV>
+    template <int IXY>
     static CLAW2_DEV void rpt2(int, const double (&asdq)[MEQN], const double (&)[NROE],
                                                 const double* a1p, const double* a2p, const double* a3p,
-                                                const double*, double (&bm)[MEQN], double (&bp)[MEQN], DV& dv)
+                                                const double*, double (&bm)[MEQN], double (&bp)[MEQN])
     {
         constexpr int mu = Dir<IXY>::MU, mv = Dir<IXY>::MV;
         const double cm = a1p[1], cp = a3p[1];
         const double zm = a1p[0] * a1p[1];
         const double zz = a2p[0] * a2p[1];
         const double zp = a3p[0] * a3p[1];
-        const double b1 = dv(-asdq[0] + zz * asdq[mv], zm + zz);
-        const double b2 = dv(asdq[0] + zz * asdq[mv], zz + zp);
+        const double b1 = (-asdq[0] + zz * asdq[mv]) / (zm + zz);
+        const double b2 = (asdq[0] + zz * asdq[mv]) / (zz + zp);
         bm[0] = cm * b1 * zm; bm[mu] = 0.0; bm[mv] = -cm * b1;
         bp[0] = cp * b2 * zp; bp[mu] = 0.0; bp[mv] = cp * b2;
     }
@@ -306,54 +300,54 @@ struct RpVcAcoustics {
 struct RpShallow {
     static constexpr int MEQN = 3, MW = 3, MAUX = 0, NROE = 3;   // ubar, vbar, cbar
 
-    template <int IXY, class DV>
+    template <int IXY>
     static CLAW2_DEV void rpn2(const double (&qL)[MEQN], const double (&qR)[MEQN],
                                                 const double*, const double*, const double* prm,
                                                 double (&wave)[MW][MEQN], double (&s)[MW],
                                                 double (&amdq)[MEQN], double (&apdq)[MEQN],
-                                                double (&roe)[NROE], DV& dv)
+                                                double (&roe)[NROE])
     {
         constexpr int mu = Dir<IXY>::MU, mv = Dir<IXY>::MV;
         const double grav = prm[0];
         const double hl = qL[0], hr = qR[0];
-        const double hsqrtl = dv.sqrt(hl), hsqrtr = dv.sqrt(hr);
+        const double hsqrtl = sqrt(hl), hsqrtr = sqrt(hr);
         const double hsq2 = hsqrtl + hsqrtr;
-        const double ubar = dv(dv(qL[mu], hsqrtl) + dv(qR[mu], hsqrtr), hsq2);
-        const double vbar = dv(dv(qL[mv], hsqrtl) + dv(qR[mv], hsqrtr), hsq2);
+        const double ubar = (qL[mu] / hsqrtl + qR[mu] / hsqrtr) / hsq2;
+        const double vbar = (qL[mv] / hsqrtl + qR[mv] / hsqrtr) / hsq2;
         const double hbar = 0.5 * (hl + hr);
-        const double cbar = dv.sqrt(grav * hbar);
+        const double cbar = sqrt(grav * hbar);
         const double delta1 = hr - hl;
         const double delta2 = qR[mu] - qL[mu];
         const double delta3 = qR[mv] - qL[mv];
-        const double a1 = dv((ubar + cbar) * delta1 - delta2, 2.0 * cbar);
+        const double a1 = ((ubar + cbar) * delta1 - delta2) / (2.0 * cbar);
         const double a2 = delta3 - vbar * delta1;
-        const double a3 = dv(delta2 - (ubar - cbar) * delta1, 2.0 * cbar);
+        const double a3 = (delta2 - (ubar - cbar) * delta1) / (2.0 * cbar);
         roe[0] = ubar; roe[1] = vbar; roe[2] = cbar;
         wave[0][0] = a1; wave[0][mu] = a1 * (ubar - cbar); wave[0][mv] = a1 * vbar; s[0] = ubar - cbar;
         wave[1][0] = 0.0; wave[1][mu] = 0.0; wave[1][mv] = a2; s[1] = ubar;
         wave[2][0] = a3; wave[2][mu] = a3 * (ubar + cbar); wave[2][mv] = a3 * vbar; s[2] = ubar + cbar;
 
-        const double s0 = dv(qL[mu], hl) - dv.sqrt(grav * hl);
+        const double s0 = qL[mu] / hl - sqrt(grav * hl);
         if (s0 >= 0.0 && s[0] > 0.0) {
             amdq[0] = 0.0; amdq[1] = 0.0; amdq[2] = 0.0;
         } else {
             const double h1 = hl + wave[0][0];
             const double hu1 = qL[mu] + wave[0][mu];
-            const double s1 = dv(hu1, h1) - dv.sqrt(grav * h1);
+            const double s1 = hu1 / h1 - sqrt(grav * h1);
             double sfract;
-            if (s0 < 0.0 && s1 > 0.0) sfract = dv(s0 * (s1 - s[0]), s1 - s0);
+            if (s0 < 0.0 && s1 > 0.0) sfract = s0 * (s1 - s[0]) / (s1 - s0);
             else if (s[0] < 0.0) sfract = s[0];
             else sfract = 0.0;
 #pragma unroll
             for (int m = 0; m < MEQN; m++) amdq[m] = sfract * wave[0][m];
             if (s[1] < 0.0) {
                 amdq[mv] = amdq[mv] + s[1] * wave[1][mv];
-                const double s3 = dv(qR[mu], hr) + dv.sqrt(grav * hr);
+                const double s3 = qR[mu] / hr + sqrt(grav * hr);
                 const double h2 = hr - wave[2][0];
                 const double hu2 = qR[mu] - wave[2][mu];
-                const double s2 = dv(hu2, h2) + dv.sqrt(grav * h2);
+                const double s2 = hu2 / h2 + sqrt(grav * h2);
                 bool add3 = true;
-                if (s2 < 0.0 && s3 > 0.0) sfract = dv(s2 * (s3 - s[2]), s3 - s2);
+                if (s2 < 0.0 && s3 > 0.0) sfract = s2 * (s3 - s[2]) / (s3 - s2);
                 else if (s[2] < 0.0) sfract = s[2];
                 else add3 = false;
                 if (add3) {
@@ -374,16 +368,16 @@ struct RpShallow {
         apdq[mv] = dfv - amdq[mv];
     }
 
-    template <int IXY, class DV>
+    template <int IXY>
     static CLAW2_DEV void rpt2(int, const double (&asdq)[MEQN], const double (&roe)[NROE],
                                                 const double*, const double*, const double*,
-                                                const double*, double (&bm)[MEQN], double (&bp)[MEQN], DV& dv)
+                                                const double*, double (&bm)[MEQN], double (&bp)[MEQN])
     {
         constexpr int mu = Dir<IXY>::MU, mv = Dir<IXY>::MV;
         const double u = roe[0], v = roe[1], c = roe[2];
-        const double a1 = dv((v + c) * asdq[0] - asdq[mv], 2.0 * c);
+        const double a1 = ((v + c) * asdq[0] - asdq[mv]) / (2.0 * c);
         const double a2 = asdq[mu] - u * asdq[0];
-        const double a3 = dv(asdq[mv] - (v - c) * asdq[0], 2.0 * c);
+        const double a3 = (asdq[mv] - (v - c) * asdq[0]) / (2.0 * c);
         double wb[3][3];
         wb[0][0] = a1; wb[0][mu] = a1 * u; wb[0][mv] = a1 * (v - c);
         wb[1][0] = 0.0; wb[1][mu] = a2; wb[1][mv] = 0.0;
