@@ -15,6 +15,7 @@
 #include "../../include/claw2.h"
 #include "claw2_kernels.cuh"
 #include "claw2_light.cuh"
+#include "claw2_lean.cuh"
 
 namespace claw2 {
 
@@ -48,6 +49,28 @@ __global__ void __launch_bounds__(256, CLAW2_LIGHT_MINB) light_step_kernel(StepA
     const TileId t{(int)blockIdx.x, (int)blockIdx.y, (int)gridDim.x, (int)gridDim.y,
                    (int)(blockIdx.y * gridDim.x + blockIdx.x), (int)(gridDim.x * gridDim.y)};
     light_tile_at<RP, 29, 29, 256>(a, ctx, t);
+}
+
+// The dense-wave solvers without aux arrays (Euler, shallow water) have the
+// same data movement in a lean unsplit body (claw2_lean.cuh): shuffles
+// instead of shared-memory exchange, one block barrier per chunk.
+template <class RP> struct HasLean { static constexpr bool value = false; };
+template <> struct HasLean<RpEuler<false>> { static constexpr bool value = true; };
+template <> struct HasLean<RpEuler<true>> { static constexpr bool value = true; };
+template <> struct HasLean<RpShallow> { static constexpr bool value = true; };
+
+#ifndef CLAW2_LEAN_MINB
+#define CLAW2_LEAN_MINB 2
+#endif
+
+template <class RP>
+__global__ void __launch_bounds__(256, CLAW2_LEAN_MINB) lean_step_kernel(StepArgs a)
+{
+    extern __shared__ double smem_dyn[];
+    DevCtx ctx{smem_dyn};
+    const TileId t{(int)blockIdx.x, (int)blockIdx.y, (int)gridDim.x, (int)gridDim.y,
+                   (int)(blockIdx.y * gridDim.x + blockIdx.x), (int)(gridDim.x * gridDim.y)};
+    lean_tile_at<RP, 29, 29, 256>(a, ctx, t);
 }
 
 // Batched step: a persistent grid walks the concatenated tile list of all
@@ -285,11 +308,28 @@ int launch_light(const StepArgs& a, int nbx, int nby, cudaStream_t st)
     return cudaGetLastError() == cudaSuccess ? CLAW2_OK : CLAW2_ERR_CUDA;
 }
 
+template <class RP>
+int launch_lean(const StepArgs& a, int nbx, int nby, cudaStream_t st)
+{
+    using SM = LeanSmem<RP, 29, 29, 256>;
+    auto kern = lean_step_kernel<RP>;
+    static bool configured = false;
+    if (!configured) {
+        if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SM::bytes) != cudaSuccess)
+            return CLAW2_ERR_CUDA;
+        configured = true;
+    }
+    kern<<<dim3(nbx, nby), 256, SM::bytes, st>>>(a);
+    return cudaGetLastError() == cudaSuccess ? CLAW2_OK : CLAW2_ERR_CUDA;
+}
+
 template <class RP, bool SPLIT>
 int launch_step_t(const StepArgs& a, int nbx, int nby, cudaStream_t st)
 {
     if constexpr (!SPLIT && HasLight<RP>::value)
         if (a.capa < 0 && !a.fwave) return launch_light<RP>(a, nbx, nby, st);
+    if constexpr (!SPLIT && HasLean<RP>::value)
+        if (a.capa < 0 && !a.fwave) return launch_lean<RP>(a, nbx, nby, st);
     constexpr int TX = SPLIT ? STX : UTX, TY = SPLIT ? STY : UTY, NT = SPLIT ? SNT : UNT;
     using SM = TileSmem<RP, TX, TY, NT, SPLIT>;
     auto kern = step_kernel<RP, TX, TY, NT, SPLIT>;

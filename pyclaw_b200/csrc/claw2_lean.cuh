@@ -1,0 +1,320 @@
+// claw2_lean.cuh -- a leaner unsplit tile body for the solvers with dense
+// waves and no aux arrays (Euler 4- and 5-wave Roe, shallow-water Roe).
+//
+// Same step as step_tile_at (step2.f90:92-248 / flux2.f90:104-206) with the
+// same operations in the same order, so the results are the same values; only
+// the data movement differs, as in the acoustics body of claw2_light.cuh:
+//  - the normal solve stays in registers; for the limiter each lane takes its
+//    right neighbour's wave by warp shuffle and forms dotr = wave(k).wave(k+1);
+//    dotl of lane k is dotr of lane k-1 (one more shuffle), the same products
+//    summed in the same component order (a*b == b*a exactly);
+//  - what the cell left of an interface needs from it (dtdx*amdq, fadd and
+//    the two transverse splits) moves one lane by shuffle;
+//  - a cell's own-line contributions stay in registers; only the two
+//    cross-line terms (to the line above and below) go through a
+//    double-buffered shared array: one block barrier per chunk of lines;
+//  - the y lines read their inputs from a staged copy of the chunk's columns,
+//    loaded row-wise (coalesced) and read down columns of an odd pitch.
+#pragma once
+
+#include "claw2_kernels.cuh"
+
+namespace claw2 {
+
+// Shared memory of the lean body (doubles): the tile state, the cross-line
+// exchange (2 buffers x 2 terms x MEQN x NT), the reduction scratch and the
+// staged inputs of one chunk of y lines (MEQN fields x YR rows x YP columns).
+template <class RP, int TX, int TY, int NT> struct LeanSmem {
+    static constexpr int MEQN = RP::MEQN;
+    static constexpr int LPC = NT / 32;
+    static constexpr int QX = MEQN * TX * TY;
+    static constexpr int CX = 2 * 2 * MEQN * NT;
+    static constexpr int YR = TY + 4;            // rows j0-2 .. j0+TY+1 read by the lanes
+    static constexpr int YP = LPC | 1;           // columns c0 .. c0+LPC-1, odd pitch
+    static constexpr int YS = MEQN * YR * YP;
+    static constexpr int total = QX + CX + NT + YS;
+    static constexpr int bytes = total * 8;
+};
+
+// Copy the state of columns c0 .. c0+LPC-1, rows j0-2 .. j0+TY+1, into STG
+// with row-wise loads.  Cells outside the ghosted array are set to 0 (no lane
+// reads them).
+template <class RP, int TY, int NT, class Ctx>
+CLAW2_HD void lean_stage_y(const StepArgs& a, Ctx& ctx, const double* __restrict__ qin, double* STG, int c0, int j0)
+{
+    constexpr int MEQN = RP::MEQN;
+    using SM = LeanSmem<RP, 1, TY, NT>;
+    constexpr int YR = SM::YR, YP = SM::YP, NC = NT / 32, NPOS = YR * NC, FS = YR * YP;
+    const long long P = a.plane;
+    for (int t = ctx.tid(); t < NPOS; t += NT) {
+        const int r = t / NC, c = t - r * NC;
+        const int col = c0 + c, row = j0 - 2 + r;
+        const bool in = col >= -CLAW2_NUM_GHOST && col < a.mx + CLAW2_NUM_GHOST && row >= -CLAW2_NUM_GHOST &&
+                        row < a.my + CLAW2_NUM_GHOST;
+        const long long o = in ? qoff(a, 0, col, row) : 0;
+        double* d = STG + r * YP + c;
+#pragma unroll
+        for (int m = 0; m < MEQN; m++) d[m * FS] = in ? qin[o + m * P] : 0.0;
+    }
+}
+
+// One chunk of one sweep direction (arguments as in sweep_chunk); CXb is the
+// half of the exchange array this chunk uses.
+template <class RP, int IXY, int TX, int TY, int NT, class Ctx>
+CLAW2_HD void lean_chunk(const StepArgs& a, Ctx& ctx, const double* __restrict__ qin, double* Qx, double* CXb,
+                         const double* STG, int i0, int j0, int line, int cfirst, int clast, bool lineok,
+                         double dtn, double dtt, double& cflm)
+{
+    constexpr int MEQN = RP::MEQN, MW = RP::MW, NROE = RP::NROE;
+    using SM = LeanSmem<RP, TX, TY, NT>;
+    constexpr int YR = SM::YR, YP = SM::YP;
+    constexpr int NCELL = IXY == 1 ? TX : TY;
+    constexpr int NSLOT = NCELL + 3;
+    const int tid = ctx.tid();
+    const int slot = tid & 31;
+    const int len = IXY == 1 ? a.mx : a.my;
+    const int k = (IXY == 1 ? i0 : j0) - 1 + slot;
+    const bool ifok = lineok && slot < NSLOT && k <= len + 1;
+    const bool lim = ifok && slot >= 1 && slot <= NSLOT - 2 && k >= 0 && k <= len;
+    const long long P = a.plane;
+
+    // ---------------- normal solve ----------------
+    double wave[MW][MEQN], s[MW], amdq[MEQN], apdq[MEQN], roe[NROE];
+#pragma unroll
+    for (int p = 0; p < MW; p++) {
+        s[p] = 0.0;
+#pragma unroll
+        for (int m = 0; m < MEQN; m++) wave[p][m] = 0.0;
+    }
+#pragma unroll
+    for (int m = 0; m < MEQN; m++) { amdq[m] = 0.0; apdq[m] = 0.0; }
+#pragma unroll
+    for (int r = 0; r < NROE; r++) roe[r] = 0.0;
+    if (ifok) {
+        double qL[MEQN], qR[MEQN];
+        if constexpr (IXY == 2) {
+            const int sc = line - cfirst;       // this line's column in STG
+#pragma unroll
+            for (int m = 0; m < MEQN; m++) {
+                qL[m] = STG[(m * YR + slot) * YP + sc];
+                qR[m] = STG[(m * YR + slot + 1) * YP + sc];
+            }
+        } else {
+            const long long oL = qoff(a, 0, k - 1, line);
+#pragma unroll
+            for (int m = 0; m < MEQN; m++) {
+                qL[m] = qin[oL + m * P];
+                qR[m] = qin[oL + 1 + m * P];
+            }
+        }
+        const double noaux[1] = {0.0};
+        RP::template rpn2<IXY>(qL, qR, noaux, noaux, a.prm, wave, s, amdq, apdq, roe);
+    }
+
+    // ---------------- CFL, limiter, second-order corrections ----------------
+    if (lim) {
+#pragma unroll
+        for (int p = 0; p < MW; p++) {
+            const double c1 = dtn * s[p], c2 = -dtn * s[p];
+            cflm = cflm > c1 ? cflm : c1;
+            cflm = cflm > c2 ? cflm : c2;
+        }
+    }
+    double cqxx[MEQN], fadd[MEQN];
+#pragma unroll
+    for (int m = 0; m < MEQN; m++) { cqxx[m] = 0.0; fadd[m] = 0.0; }
+    if (a.order == 2) {                       // uniform: every lane takes part in the shuffles
+        const double dtdxave = 0.5 * (dtn + dtn);
+#pragma unroll
+        for (int p = 0; p < MW; p++) {
+            double dotr = 0.0;
+#pragma unroll
+            for (int m = 0; m < MEQN; m++) dotr = dotr + wave[p][m] * ctx.shfl_down(wave[p][m]);
+            const double dotl = ctx.shfl_up(dotr);
+            if (lim) {
+                double wv[MEQN];
+#pragma unroll
+                for (int m = 0; m < MEQN; m++) wv[m] = wave[p][m];
+                const int meth = a.mthlim[p];
+                if (a.limit_any && meth != 0) {
+                    double wnorm2 = 0.0;
+#pragma unroll
+                    for (int m = 0; m < MEQN; m++) wnorm2 = wnorm2 + wv[m] * wv[m];
+                    if (wnorm2 != 0.0) {
+                        const double phi = philim(wnorm2, s[p] > 0.0 ? dotl : dotr, meth);
+#pragma unroll
+                        for (int m = 0; m < MEQN; m++) wv[m] = phi * wv[m];
+                    }
+                }
+                const double as = fabs(s[p]);
+                const double f = as * (1.0 - as * dtdxave);
+#pragma unroll
+                for (int m = 0; m < MEQN; m++) cqxx[m] = (p == 0) ? f * wv[m] : cqxx[m] + f * wv[m];
+            }
+        }
+#pragma unroll
+        for (int m = 0; m < MEQN; m++) fadd[m] = 0.5 * cqxx[m];
+    }
+
+    // ---------------- transverse splits ----------------
+    double bmL[MEQN], bpL[MEQN], bmR[MEQN], bpR[MEQN];
+#pragma unroll
+    for (int m = 0; m < MEQN; m++) { bmL[m] = 0.0; bpL[m] = 0.0; bmR[m] = 0.0; bpR[m] = 0.0; }
+    if (lim && a.trans > 0) {
+        const bool cor = a.order == 2 && a.trans == 2;
+        double A[MEQN], Pf[MEQN];
+#pragma unroll
+        for (int m = 0; m < MEQN; m++) {
+            A[m] = cor ? amdq[m] + cqxx[m] : amdq[m];
+            Pf[m] = cor ? apdq[m] - cqxx[m] : apdq[m];
+        }
+        const double noaux[1] = {0.0};
+        RP::template rpt2<IXY>(1, A, roe, noaux, noaux, noaux, a.prm, bmL, bpL);
+        RP::template rpt2<IXY>(2, Pf, roe, noaux, noaux, noaux, a.prm, bmR, bpR);
+    }
+
+    // ---------------- the slice's contributions to cell k ----------------
+    // what interface k+1 hands to its left cell (this lane's cell k)
+    const double hl = 0.5 * dtn;
+    double y0[MEQN], y1[MEQN], y2[MEQN], y3[MEQN];
+#pragma unroll
+    for (int m = 0; m < MEQN; m++) {
+        y0[m] = ctx.shfl_down(lim ? dtn * amdq[m] : 0.0);
+        y1[m] = ctx.shfl_down(lim ? fadd[m] : 0.0);
+        y2[m] = ctx.shfl_down(lim ? hl * bmL[m] : 0.0);
+        y3[m] = ctx.shfl_down(lim ? hl * bpL[m] : 0.0);
+    }
+    const bool cellok = lim && slot <= NCELL && k < len;
+    const bool trans = a.trans > 0;
+    double C0[MEQN], C1[MEQN], C2[MEQN], C3[MEQN], C4[MEQN];
+#pragma unroll
+    for (int m = 0; m < MEQN; m++) {
+        C0[m] = 0.0; C1[m] = 0.0; C2[m] = 0.0; C3[m] = 0.0; C4[m] = 0.0;
+    }
+    if (cellok) {
+        const double hr = 0.5 * dtn;
+#pragma unroll
+        for (int m = 0; m < MEQN; m++) {
+            const double qadd = (0.0 - dtn * apdq[m]) - y0[m];
+            const double dF = y1[m] - fadd[m];
+            const double g1 = (0.0 - y2[m]) - hr * bmR[m];
+            const double g2 = (0.0 - y3[m]) - hr * bpR[m];
+            C0[m] = dtt * g2;
+            C1[m] = qadd;
+            C2[m] = dtn * dF;
+            C3[m] = dtt * (g2 - g1);
+            C4[m] = dtt * g1;
+        }
+    }
+#pragma unroll
+    for (int m = 0; m < MEQN; m++) {
+        CXb[m * NT + tid] = C0[m];
+        CXb[(MEQN + m) * NT + tid] = C4[m];
+    }
+    ctx.sync();
+
+    // ---------------- combine slices line-1, line, line+1 per cell ----------------
+    if (cellok) {
+        auto qx = [&](int m, int kk, int ll) -> double& {
+            const int ci = IXY == 1 ? kk : ll, cj = IXY == 1 ? ll : kk;
+            return Qx[(m * TY + (cj - j0)) * TX + (ci - i0)];
+        };
+        auto qi = [&](int m, int kk, int ll) -> double {
+            return IXY == 1 ? qin[qoff(a, m, kk, ll)] : qx(m, kk, ll);
+        };
+        auto in_tile_line = [&](int ll) {
+            return IXY == 1 ? (ll >= j0 && ll < j0 + TY && ll < a.my) : (ll >= i0 && ll < i0 + TX && ll < a.mx);
+        };
+        const int up = tid - 32, dn = tid + 32;     // the lanes of lines line-1 and line+1
+        if (in_tile_line(line)) {
+#pragma unroll
+            for (int m = 0; m < MEQN; m++) {
+                double v;
+                if (line == cfirst) v = qx(m, k, line);                 // has up(line-1) already
+                else {
+                    v = qi(m, k, line);
+                    if (trans) v = v + CXb[m * NT + up];
+                }
+                if (IXY == 1) {
+                    v = v + C1[m] - C2[m];
+                    if (trans) v = v - C3[m];
+                } else {
+                    v = v + (trans ? (C1[m] - C2[m] - C3[m]) : (C1[m] - C2[m]));
+                }
+                if (trans && line != clast) v = v - CXb[(MEQN + m) * NT + dn];
+                qx(m, k, line) = v;
+            }
+        }
+        if (line == clast && in_tile_line(line + 1)) {
+#pragma unroll
+            for (int m = 0; m < MEQN; m++) {
+                double v = qi(m, k, line + 1);
+                if (trans) v = v + C0[m];
+                qx(m, k, line + 1) = v;
+            }
+        }
+        if (trans && line == cfirst && in_tile_line(line - 1)) {
+#pragma unroll
+            for (int m = 0; m < MEQN; m++) qx(m, k, line - 1) = qx(m, k, line - 1) - C4[m];
+        }
+    }
+}
+
+// Whole-tile unsplit step with the lean body (the caller checks that the
+// problem has no capacity function and no f-waves).
+template <class RP, int TX, int TY, int NT, class Ctx>
+CLAW2_HD void lean_tile_at(const StepArgs& a, Ctx& ctx, const TileId& tile)
+{
+    constexpr int MEQN = RP::MEQN;
+    using SM = LeanSmem<RP, TX, TY, NT>;
+    constexpr int LPC = NT / 32;
+    static_assert(TX + 3 <= 32 && TY + 3 <= 32, "tile too wide for one 32-lane line");
+    static_assert(RP::MAUX == 0, "the lean body serves the solvers without aux arrays");
+    double* Qx = ctx.smem();
+    double* CX = Qx + SM::QX;
+    double* red = CX + SM::CX;
+    double* STG = red + NT;
+    const int tid = ctx.tid();
+    const int warp = tid >> 5;
+    const int i0 = tile.bx * TX, j0 = tile.by * TY;
+    const double* qin = a.qin;
+    double* qout = a.qout;
+    double dt = a.dt;
+    if (a.ctrl) {
+        if (a.ctrl->done) return;                  // uniform across the grid
+        dt = a.ctrl->dt;
+        const int cur = a.ctrl->cur;
+        qin = cur ? a.q1 : a.q0;
+        qout = cur ? a.q0 : a.q1;
+    }
+    const double dtdx = dt / a.dx, dtdy = dt / a.dy;
+    double cflm = 0.0;
+    int chunk = 0;
+    {
+        const int first = j0 - 1;
+        const int last = (j0 + TY < a.my) ? j0 + TY : a.my;
+        for (int c0 = first; c0 <= last; c0 += LPC, chunk++) {
+            const int line = c0 + warp;
+            const int clast = (c0 + LPC - 1 < last) ? c0 + LPC - 1 : last;
+            lean_chunk<RP, 1, TX, TY, NT>(a, ctx, qin, Qx, CX + (chunk & 1) * 2 * MEQN * NT, nullptr, i0, j0, line,
+                                          c0, clast, line <= last, dtdx, dtdy, cflm);
+        }
+    }
+    {
+        const int first = i0 - 1;
+        const int last = (i0 + TX < a.mx) ? i0 + TX : a.mx;
+        for (int c0 = first; c0 <= last; c0 += LPC, chunk++) {
+            const int line = c0 + warp;
+            const int clast = (c0 + LPC - 1 < last) ? c0 + LPC - 1 : last;
+            // the previous chunk's barrier has passed: no lane still reads STG
+            lean_stage_y<RP, TY, NT>(a, ctx, qin, STG, c0, j0);
+            ctx.sync();
+            lean_chunk<RP, 2, TX, TY, NT>(a, ctx, qin, Qx, CX + (chunk & 1) * 2 * MEQN * NT, STG, i0, j0, line, c0,
+                                          clast, line <= last, dtdy, dtdx, cflm);
+        }
+    }
+    ctx.sync();
+    finish_tile<MEQN, TX, TY, NT>(a, ctx, tile, Qx, TX * TY, red, qout, i0, j0, cflm, dt);
+}
+
+}  // namespace claw2

@@ -55,6 +55,30 @@ def test_step_bit_identical_to_oracle(orc, name, mx, my, tr, order, bcl, bcu):
     assert np.array_equal(out, ref), "ghost cells differ from the boundary fill of the new state"
 
 
+LIMITER_CASES = [(name, lim, order, tr) for name in ("euler4", "shallow") for lim in (0, 1, 2, 3, 5)
+                 for order, tr in ((2, 2), (2, 1))]
+LIMITER_CASES += [("euler4", 4, 1, 2), ("shallow", 2, 1, 1), ("euler5", 2, 2, 2), ("euler5", 1, 1, 0)]
+
+
+@pytest.mark.parametrize("name,lim,order,tr", LIMITER_CASES)
+def test_unsplit_limiters_bit_identical_to_oracle(orc, name, lim, order, tr):
+    """Every limiter id (0 = none, 1-5) and first order through the unsplit
+    bodies of the dense-wave solvers, on a grid of several partial tiles."""
+    mx, my = 75, 62
+    p = H.problem(name, mx, my, tr, order=order, mthlim=(lim,), bcl=(1, 3), bcu=(3, 1))
+    q, aux = H.init_fields(p, seed=lim * 13 + order + tr)
+    qbc = orc.new_qbc(p, q)
+    orc.fill_ghosts(p, qbc)
+    dt = 0.25 / max(mx, my)
+    ref = qbc.copy(order="F")
+    cfl_ref = orc.step_hyperbolic(p, ref, None, dt)
+    out, cfl = H.dev_step(p, qbc, None, dt)
+    assert np.array_equal(out[I], ref[I]), np.nanmax(np.abs(out[I] - ref[I]))
+    assert cfl == cfl_ref
+    orc.fill_ghosts(p, ref)
+    assert np.array_equal(out, ref)
+
+
 def test_nonfinite_state_is_reported(orc):
     p = H.problem("euler4", 40, 40, 2)
     q, _ = H.init_fields(p)
