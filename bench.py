@@ -472,7 +472,7 @@ def run_ours(args, world, rank, local):
     avg_kernel_s = t_dev / args.steps
     achieved = alg_bytes / avg_kernel_s / 1e9
     traffic = None
-    tpath = os.path.join(ROOT, "profiles", "step_kernel_euler1280x320.md")
+    tpath = os.path.join(ROOT, "profiles", "lean_step_kernel_euler1280x320.md")
     if os.path.exists(tpath):            # dram read+write bytes of one launch, from the ncu capture
         with open(tpath) as f:
             for ln in f:

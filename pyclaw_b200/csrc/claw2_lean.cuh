@@ -13,8 +13,10 @@
 //  - a cell's own-line contributions stay in registers; only the two
 //    cross-line terms (to the line above and below) go through a
 //    double-buffered shared array: one block barrier per chunk of lines;
-//  - the y lines read their inputs from a staged copy of the chunk's columns,
-//    loaded row-wise (coalesced) and read down columns of an odd pitch.
+//  - the tile's whole input halo (rows j0-2..j0+TY+1, columns i0-2..i0+TX+1)
+//    is staged in shared memory once, with coalesced row-wise loads all in
+//    flight together; x lines read rows of it and y lines read down its
+//    columns, whose odd pitch keeps those reads free of bank conflicts.
 #pragma once
 
 #include "claw2_kernels.cuh"
@@ -23,51 +25,53 @@ namespace claw2 {
 
 // Shared memory of the lean body (doubles): the tile state, the cross-line
 // exchange (2 buffers x 2 terms x MEQN x NT), the reduction scratch and the
-// staged inputs of one chunk of y lines (MEQN fields x YR rows x YP columns).
+// staged input halo (MEQN fields x TR rows x TP columns).
 template <class RP, int TX, int TY, int NT> struct LeanSmem {
     static constexpr int MEQN = RP::MEQN;
-    static constexpr int LPC = NT / 32;
     static constexpr int QX = MEQN * TX * TY;
     static constexpr int CX = 2 * 2 * MEQN * NT;
-    static constexpr int YR = TY + 4;            // rows j0-2 .. j0+TY+1 read by the lanes
-    static constexpr int YP = LPC | 1;           // columns c0 .. c0+LPC-1, odd pitch
-    static constexpr int YS = MEQN * YR * YP;
-    static constexpr int total = QX + CX + NT + YS;
+    static constexpr int TR = TY + 4;            // rows j0-2 .. j0+TY+1
+    static constexpr int TP = TX + 4;            // columns i0-2 .. i0+TX+1
+    static_assert(TP % 2 == 1, "the halo pitch must be odd");
+    static constexpr int HS = MEQN * TR * TP;
+    static constexpr int total = QX + CX + NT + HS;
     static constexpr int bytes = total * 8;
 };
 
-// Copy the state of columns c0 .. c0+LPC-1, rows j0-2 .. j0+TY+1, into STG
-// with row-wise loads.  Cells outside the ghosted array are set to 0 (no lane
-// reads them).
-template <class RP, int TY, int NT, class Ctx>
-CLAW2_HD void lean_stage_y(const StepArgs& a, Ctx& ctx, const double* __restrict__ qin, double* STG, int c0, int j0)
+// Copy the tile's input halo into H: H[(m*TR + r)*TP + c] = q(m, i0-2+c, j0-2+r).
+// Cells outside the ghosted array are set to 0 (no lane reads them).
+template <class RP, int TX, int TY, int NT, class Ctx>
+CLAW2_HD void lean_stage(const StepArgs& a, Ctx& ctx, const double* __restrict__ qin, double* H, int i0, int j0)
 {
     constexpr int MEQN = RP::MEQN;
-    using SM = LeanSmem<RP, 1, TY, NT>;
-    constexpr int YR = SM::YR, YP = SM::YP, NC = NT / 32, NPOS = YR * NC, FS = YR * YP;
+    using SM = LeanSmem<RP, TX, TY, NT>;
+    constexpr int TR = SM::TR, TP = SM::TP, NPOS = TR * TP, FS = TR * TP;
     const long long P = a.plane;
     for (int t = ctx.tid(); t < NPOS; t += NT) {
-        const int r = t / NC, c = t - r * NC;
-        const int col = c0 + c, row = j0 - 2 + r;
+        const int r = t / TP, c = t - r * TP;
+        const int col = i0 - 2 + c, row = j0 - 2 + r;
         const bool in = col >= -CLAW2_NUM_GHOST && col < a.mx + CLAW2_NUM_GHOST && row >= -CLAW2_NUM_GHOST &&
                         row < a.my + CLAW2_NUM_GHOST;
         const long long o = in ? qoff(a, 0, col, row) : 0;
-        double* d = STG + r * YP + c;
 #pragma unroll
-        for (int m = 0; m < MEQN; m++) d[m * FS] = in ? qin[o + m * P] : 0.0;
+        for (int m = 0; m < MEQN; m++) H[m * FS + t] = in ? qin[o + m * P] : 0.0;
     }
 }
 
 // One chunk of one sweep direction (arguments as in sweep_chunk); CXb is the
 // half of the exchange array this chunk uses.
 template <class RP, int IXY, int TX, int TY, int NT, class Ctx>
-CLAW2_HD void lean_chunk(const StepArgs& a, Ctx& ctx, const double* __restrict__ qin, double* Qx, double* CXb,
-                         const double* STG, int i0, int j0, int line, int cfirst, int clast, bool lineok,
-                         double dtn, double dtt, double& cflm)
+CLAW2_HD void lean_chunk(const StepArgs& a, Ctx& ctx, const double* H, double* Qx, double* CXb, int i0, int j0,
+                         int line, int cfirst, int clast, bool lineok, double dtn, double dtt, double& cflm)
 {
     constexpr int MEQN = RP::MEQN, MW = RP::MW, NROE = RP::NROE;
     using SM = LeanSmem<RP, TX, TY, NT>;
-    constexpr int YR = SM::YR, YP = SM::YP;
+    constexpr int TR = SM::TR, TP = SM::TP;
+    // the staged input of cell (kk along the slice, ll across it)
+    auto hq = [&](int m, int kk, int ll) -> double {
+        return IXY == 1 ? H[(m * TR + (ll - j0 + 2)) * TP + (kk - i0 + 2)]
+                        : H[(m * TR + (kk - j0 + 2)) * TP + (ll - i0 + 2)];
+    };
     constexpr int NCELL = IXY == 1 ? TX : TY;
     constexpr int NSLOT = NCELL + 3;
     const int tid = ctx.tid();
@@ -76,7 +80,6 @@ CLAW2_HD void lean_chunk(const StepArgs& a, Ctx& ctx, const double* __restrict__
     const int k = (IXY == 1 ? i0 : j0) - 1 + slot;
     const bool ifok = lineok && slot < NSLOT && k <= len + 1;
     const bool lim = ifok && slot >= 1 && slot <= NSLOT - 2 && k >= 0 && k <= len;
-    const long long P = a.plane;
 
     // ---------------- normal solve ----------------
     double wave[MW][MEQN], s[MW], amdq[MEQN], apdq[MEQN], roe[NROE];
@@ -92,20 +95,10 @@ CLAW2_HD void lean_chunk(const StepArgs& a, Ctx& ctx, const double* __restrict__
     for (int r = 0; r < NROE; r++) roe[r] = 0.0;
     if (ifok) {
         double qL[MEQN], qR[MEQN];
-        if constexpr (IXY == 2) {
-            const int sc = line - cfirst;       // this line's column in STG
 #pragma unroll
-            for (int m = 0; m < MEQN; m++) {
-                qL[m] = STG[(m * YR + slot) * YP + sc];
-                qR[m] = STG[(m * YR + slot + 1) * YP + sc];
-            }
-        } else {
-            const long long oL = qoff(a, 0, k - 1, line);
-#pragma unroll
-            for (int m = 0; m < MEQN; m++) {
-                qL[m] = qin[oL + m * P];
-                qR[m] = qin[oL + 1 + m * P];
-            }
+        for (int m = 0; m < MEQN; m++) {
+            qL[m] = hq(m, k - 1, line);
+            qR[m] = hq(m, k, line);
         }
         const double noaux[1] = {0.0};
         RP::template rpn2<IXY>(qL, qR, noaux, noaux, a.prm, wave, s, amdq, apdq, roe);
@@ -219,9 +212,7 @@ CLAW2_HD void lean_chunk(const StepArgs& a, Ctx& ctx, const double* __restrict__
             const int ci = IXY == 1 ? kk : ll, cj = IXY == 1 ? ll : kk;
             return Qx[(m * TY + (cj - j0)) * TX + (ci - i0)];
         };
-        auto qi = [&](int m, int kk, int ll) -> double {
-            return IXY == 1 ? qin[qoff(a, m, kk, ll)] : qx(m, kk, ll);
-        };
+        auto qi = [&](int m, int kk, int ll) -> double { return IXY == 1 ? hq(m, kk, ll) : qx(m, kk, ll); };
         auto in_tile_line = [&](int ll) {
             return IXY == 1 ? (ll >= j0 && ll < j0 + TY && ll < a.my) : (ll >= i0 && ll < i0 + TX && ll < a.mx);
         };
@@ -273,7 +264,7 @@ CLAW2_HD void lean_tile_at(const StepArgs& a, Ctx& ctx, const TileId& tile)
     double* Qx = ctx.smem();
     double* CX = Qx + SM::QX;
     double* red = CX + SM::CX;
-    double* STG = red + NT;
+    double* H = red + NT;
     const int tid = ctx.tid();
     const int warp = tid >> 5;
     const int i0 = tile.bx * TX, j0 = tile.by * TY;
@@ -290,14 +281,16 @@ CLAW2_HD void lean_tile_at(const StepArgs& a, Ctx& ctx, const TileId& tile)
     const double dtdx = dt / a.dx, dtdy = dt / a.dy;
     double cflm = 0.0;
     int chunk = 0;
+    lean_stage<RP, TX, TY, NT>(a, ctx, qin, H, i0, j0);
+    ctx.sync();
     {
         const int first = j0 - 1;
         const int last = (j0 + TY < a.my) ? j0 + TY : a.my;
         for (int c0 = first; c0 <= last; c0 += LPC, chunk++) {
             const int line = c0 + warp;
             const int clast = (c0 + LPC - 1 < last) ? c0 + LPC - 1 : last;
-            lean_chunk<RP, 1, TX, TY, NT>(a, ctx, qin, Qx, CX + (chunk & 1) * 2 * MEQN * NT, nullptr, i0, j0, line,
-                                          c0, clast, line <= last, dtdx, dtdy, cflm);
+            lean_chunk<RP, 1, TX, TY, NT>(a, ctx, H, Qx, CX + (chunk & 1) * 2 * MEQN * NT, i0, j0, line, c0, clast,
+                                          line <= last, dtdx, dtdy, cflm);
         }
     }
     {
@@ -306,11 +299,8 @@ CLAW2_HD void lean_tile_at(const StepArgs& a, Ctx& ctx, const TileId& tile)
         for (int c0 = first; c0 <= last; c0 += LPC, chunk++) {
             const int line = c0 + warp;
             const int clast = (c0 + LPC - 1 < last) ? c0 + LPC - 1 : last;
-            // the previous chunk's barrier has passed: no lane still reads STG
-            lean_stage_y<RP, TY, NT>(a, ctx, qin, STG, c0, j0);
-            ctx.sync();
-            lean_chunk<RP, 2, TX, TY, NT>(a, ctx, qin, Qx, CX + (chunk & 1) * 2 * MEQN * NT, STG, i0, j0, line, c0,
-                                          clast, line <= last, dtdy, dtdx, cflm);
+            lean_chunk<RP, 2, TX, TY, NT>(a, ctx, H, Qx, CX + (chunk & 1) * 2 * MEQN * NT, i0, j0, line, c0, clast,
+                                          line <= last, dtdy, dtdx, cflm);
         }
     }
     ctx.sync();
