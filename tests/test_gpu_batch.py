@@ -70,3 +70,28 @@ def test_batch_variants_agree():
     for r in results[1:]:
         for a, b in zip(results[0], r):
             assert np.array_equal(a, b)
+
+
+def test_sharded_batch_shares_equal_the_whole_batch():
+    """Each rank's share of a batch (pyclaw_b200.partition.ShardedBatch with
+    the GPU BatchSolver), stepped here one share after the other on this GPU,
+    gives every instance bit for bit the state of the unsharded batch."""
+    from pyclaw_b200 import partition
+    from pyclaw_b200.batch import BatchSolver
+    prob, insts = bench.batched_vc_config(n=9, seed=11, nmin=20, nmax=120)
+    dts = [i["dt"] for i in insts]
+    whole = BatchSolver(prob, insts)
+    whole.init_controls(dts, max_steps=25)
+    whole.advance_graph(25, chunk=10)
+    seen = set()
+    for rank in range(3):
+        sb = partition.ShardedBatch(prob, insts, rank, 3)
+        sb.init_controls(dts, max_steps=25)
+        sb.advance_graph(25, chunk=10)
+        for k, q, ns, t in sb.local_results():
+            seen.add(k)
+            assert np.array_equal(q, whole.solution(k)), k
+            assert ns == whole.controls()[k].numsteps and t == whole.controls()[k].t
+        sb.close()
+    assert seen == set(range(len(insts)))
+    whole.close()
