@@ -73,8 +73,52 @@ __global__ void __launch_bounds__(256, CLAW2_LEAN_MINB) lean_step_kernel(StepArg
     lean_tile_at<RP, 29, 29, 256>(a, ctx, t);
 }
 
+// Instance of tile t: the last one with tile_begin <= t (binary search).
+__device__ __forceinline__ int batch_instance_of(const claw2_batch_instance* __restrict__ inst, int ninst, int t)
+{
+    int lo = 0, hi = ninst - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(&inst[mid].tile_begin) <= t) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// Ask L2 for the input halo of tile t (rows j0-2..j0+TY+1 and columns
+// i0-2..i0+TX+1, clipped to the ghosted arrays, of the current state and of
+// aux) while the CTA works on the tile before it: an instance's data is read
+// once per step, from HBM, so the tile's first loads would otherwise wait for
+// DRAM.  One prefetch per 128-byte line, spread over the CTA's threads.  The
+// addresses stay inside the instance's arrays; results do not depend on it.
+template <int MEQN, int MAUX, int TX, int TY, int NT>
+__device__ __forceinline__ void batch_prefetch_tile(const claw2_batch_instance* __restrict__ inst, int ninst, int t)
+{
+    const claw2_batch_instance& I = inst[batch_instance_of(inst, ninst, t)];
+    const claw2_control* c = I.ctrl;
+    if (c->done) return;
+    const double* q = c->cur ? I.q1 : I.q0;
+    const int lt = t - I.tile_begin;
+    const int i0 = (lt % I.nbx) * TX, j0 = (lt / I.nbx) * TY;
+    const int rlo = j0 - 2, rhi = (j0 + TY + 1 < I.my + 1) ? j0 + TY + 1 : I.my + 1;
+    const int clo = i0 - 2, chi = (i0 + TX + 1 < I.mx + 1) ? i0 + TX + 1 : I.mx + 1;
+    // byte range of one row segment, in whole 128-byte lines
+    const long long b0 = (long long)(clo + CLAW2_NUM_GHOST) * 8, b1 = (long long)(chi + CLAW2_NUM_GHOST) * 8 + 8;
+    const int l0 = (int)(b0 >> 7), nl = (int)((b1 + 127) >> 7) - l0;
+    const int nrow = rhi - rlo + 1;
+    const int items = (MEQN + MAUX) * nrow * nl;
+    for (int k = threadIdx.x; k < items; k += NT) {
+        const int line = k % nl, rf = k / nl;
+        const int r = rf % nrow, f = rf / nrow;
+        const char* base = f < MEQN ? (const char*)(q + f * I.plane) : (const char*)(I.aux + (f - MEQN) * I.plane);
+        const char* ptr = base + (long long)(rlo + r + CLAW2_NUM_GHOST) * I.ld * 8 + ((long long)(l0 + line) << 7);
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(ptr));
+    }
+}
+
 // Batched step: a persistent grid walks the concatenated tile list of all
-// instances; each tile is one step_tile_at call with that instance's buffers.
+// instances; each tile is one step_tile_at call with that instance's buffers,
+// with an L2 prefetch of the CTA's next tile issued first.
 template <class RP, int NT, int MINB, bool LIGHT>
 __global__ void __launch_bounds__(NT, MINB)
 batch_kernel(const claw2_batch_instance* __restrict__ inst, int ninst, int ntiles, StepArgs common)
@@ -82,12 +126,9 @@ batch_kernel(const claw2_batch_instance* __restrict__ inst, int ninst, int ntile
     extern __shared__ double smem_dyn[];
     DevCtx ctx{smem_dyn};
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-        int lo = 0, hi = ninst - 1;                 // last instance with tile_begin <= t
-        while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (__ldg(&inst[mid].tile_begin) <= t) lo = mid;
-            else hi = mid - 1;
-        }
+        if (t + (int)gridDim.x < ntiles)
+            batch_prefetch_tile<RP::MEQN, RP::MAUX, 29, 29, NT>(inst, ninst, t + (int)gridDim.x);
+        const int lo = batch_instance_of(inst, ninst, t);
         const claw2_batch_instance& I = inst[lo];
         StepArgs a = common;
         a.q0 = I.q0; a.q1 = I.q1; a.aux = I.aux; a.ctrl = I.ctrl;
