@@ -573,13 +573,19 @@ CLAW2_HD void finish_tile(const StepArgs& a, Ctx& ctx, const TileId& tile, const
         write_cell<MEQN>(a, qout, i, j, v);
     }
 
-    // ---- block CFL max (deterministic: max is exact) and last-block epilogue
-    red[tid] = bad ? -1.0 : cflm;        // CFL numbers are >= 0; -1 flags a non-finite cell
+    // ---- block CFL max (deterministic: max is exact) and last-block epilogue:
+    // warp max by shuffles, then one value per warp.  CFL numbers are >= 0; a
+    // NaN one counts as a non-finite state, and -1 flags a warp that saw one.
+    {
+        const bool nfw = ctx.warp_any(bad != 0 || cflm != cflm);
+        const double mw = ctx.warp_max(cflm);
+        if ((tid & 31) == 0) red[tid >> 5] = nfw ? -1.0 : mw;
+    }
     ctx.sync();
     if (tid == 0) {
         double mxv = 0.0;
         int nf = 0;
-        for (int t = 0; t < NT; t++) {
+        for (int t = 0; t < NT / 32; t++) {
             if (red[t] < 0.0) nf = 1;
             else mxv = mxv > red[t] ? mxv : red[t];
         }
@@ -715,6 +721,17 @@ struct DevCtx {
     // value of the lane below / above in the warp (own value at the ends)
     __device__ __forceinline__ double shfl_up(double v) const { return __shfl_up_sync(0xffffffffu, v, 1); }
     __device__ __forceinline__ double shfl_down(double v) const { return __shfl_down_sync(0xffffffffu, v, 1); }
+    // max over the warp (all lanes get it) and any-lane predicate
+    __device__ __forceinline__ double warp_max(double v) const
+    {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const double w = __shfl_xor_sync(0xffffffffu, v, o);
+            v = v > w ? v : w;
+        }
+        return v;
+    }
+    __device__ __forceinline__ bool warp_any(bool p) const { return __any_sync(0xffffffffu, p) != 0; }
 };
 #endif
 
