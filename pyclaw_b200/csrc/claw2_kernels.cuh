@@ -582,30 +582,44 @@ CLAW2_HD void finish_tile(const StepArgs& a, Ctx& ctx, const TileId& tile, const
         if ((tid & 31) == 0) red[tid >> 5] = nfw ? -1.0 : mw;
     }
     ctx.sync();
+    constexpr int NW = NT / 32;
     if (tid == 0) {
         double mxv = 0.0;
         int nf = 0;
-        for (int t = 0; t < NT / 32; t++) {
+        for (int t = 0; t < NW; t++) {
             if (red[t] < 0.0) nf = 1;
             else mxv = mxv > red[t] ? mxv : red[t];
         }
-        const int nblocks = tile.ntiles;
-        const int bid = tile.part;
-        a.partials[bid] = nf ? -1.0 : mxv;
+        a.partials[tile.part] = nf ? -1.0 : mxv;
         ctx.fence();
         const unsigned int prev = ctx.atomic_inc(a.ticket);
-        if (prev == (unsigned int)(nblocks - 1)) {
-            ctx.fence();
-            double cfl = 0.0;
-            int nonfinite = 0;
-            for (int b = 0; b < nblocks; b++) {
-                const double v = ctx.load_volatile(&a.partials[b]);
-                if (v < 0.0) nonfinite = 1;
-                else cfl = cfl > v ? cfl : v;
+        red[NW] = prev == (unsigned int)(tile.ntiles - 1) ? 1.0 : 0.0;     // this CTA arrived last
+    }
+    ctx.sync();
+    if (red[NW] != 0.0) {
+        // the last CTA reduces every CTA's partial with all its threads
+        ctx.fence();
+        double cfl = 0.0;
+        bool nonfinite = false;
+        for (int b = tid; b < tile.ntiles; b += NT) {
+            const double v = ctx.load_volatile(&a.partials[b]);
+            if (v < 0.0) nonfinite = true;
+            else cfl = cfl > v ? cfl : v;
+        }
+        const bool nfw = ctx.warp_any(nonfinite);
+        const double mw = ctx.warp_max(cfl);
+        if ((tid & 31) == 0) red[tid >> 5] = nfw ? -1.0 : mw;
+        ctx.sync();
+        if (tid == 0) {
+            cfl = 0.0;
+            int nf = 0;
+            for (int t = 0; t < NW; t++) {
+                if (red[t] < 0.0) nf = 1;
+                else cfl = cfl > red[t] ? cfl : red[t];
             }
-            if (a.ctrl && !a.ctrl_readonly) control_update(a.ctrl, cfl, nonfinite);
-            else if (a.ctrl_readonly) *a.cfl_out = nonfinite ? 1.0 / 0.0 : cfl;
-            else *a.cfl_out = nonfinite ? ctx.nan() : cfl;
+            if (a.ctrl && !a.ctrl_readonly) control_update(a.ctrl, cfl, nf);
+            else if (a.ctrl_readonly) *a.cfl_out = nf ? 1.0 / 0.0 : cfl;
+            else *a.cfl_out = nf ? ctx.nan() : cfl;
             *a.ticket = 0u;
             ctx.fence();
         }
