@@ -467,6 +467,13 @@ __global__ void __launch_bounds__(ANT, CLAW2_ADJ_MINB) adjoint_kernel(AdjArgs a)
     const int ilo = i0 == 0 ? -2 : i0, ihi = i0 + AT >= a.mx ? a.mx + 2 : i0 + AT;
     const int jlo = j0 == 0 ? -2 : j0, jhi = j0 + AT >= a.my ? a.my + 2 : j0 + AT;
     const long long P = a.plane;
+    {
+        // the lines this tile sweeps reach one cell beyond its ghost ring
+        const DevCtx ctx{nullptr};
+        prefetch_box<ANT>(ctx, q, 3, P, a.ld, a.mx, a.my, j0 - 3, j0 + AT + 2, i0 - 3, i0 + AT + 2);
+        prefetch_box<ANT>(ctx, a.aux, 2, P, a.ld, a.mx, a.my, j0 - 3, j0 + AT + 2, i0 - 3, i0 + AT + 2);
+        prefetch_box<ANT>(ctx, lin, 3, P, a.ld, a.mx, a.my, j0 - 3, j0 + AT + 2, i0 - 3, i0 + AT + 2);
+    }
 
     for (int t = tid; t < AR * AR; t += ANT) {
         const int i = i0 - 2 + t % AR, j = j0 - 2 + t / AR;

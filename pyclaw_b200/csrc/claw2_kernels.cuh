@@ -508,6 +508,32 @@ CLAW2_HD void sweep_chunk(const StepArgs& a, Ctx& ctx, const double* qin, double
     ctx.sync();
 }
 
+// Ask L2 for rows r0..r1 and columns c0..c1 (cell indices, clipped here to
+// the ghosted array) of nf planes of a device-layout array, one prefetch per
+// 128-byte line spread over the CTA's threads: a tile's x lines then find
+// their cells in L2 instead of waiting for DRAM chunk after chunk.  Only a
+// hint; no result depends on it.
+template <int NT, class Ctx>
+CLAW2_HD void prefetch_box(Ctx& ctx, const double* base, int nf, long long P, long long ld, int mx, int my, int r0,
+                           int r1, int c0, int c1)
+{
+    r0 = r0 > -CLAW2_NUM_GHOST ? r0 : -CLAW2_NUM_GHOST;
+    r1 = r1 < my + CLAW2_NUM_GHOST - 1 ? r1 : my + CLAW2_NUM_GHOST - 1;
+    c0 = c0 > -CLAW2_NUM_GHOST ? c0 : -CLAW2_NUM_GHOST;
+    c1 = c1 < mx + CLAW2_NUM_GHOST - 1 ? c1 : mx + CLAW2_NUM_GHOST - 1;
+    if (r1 < r0 || c1 < c0) return;
+    const long long b0 = (long long)(c0 + CLAW2_NUM_GHOST) * 8, b1 = (long long)(c1 + CLAW2_NUM_GHOST) * 8 + 8;
+    const int l0 = (int)(b0 >> 7), nl = (int)((b1 + 127) >> 7) - l0;
+    const int nrow = r1 - r0 + 1;
+    const int items = nf * nrow * nl;
+    for (int k = ctx.tid(); k < items; k += NT) {
+        const int line = k % nl, rf = k / nl;
+        const int r = rf % nrow, f = rf / nrow;
+        ctx.prefetch_l2((const char*)(base + f * P) + (long long)(r0 + r + CLAW2_NUM_GHOST) * ld * 8 +
+                        ((long long)(l0 + line) << 7));
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Whole-tile step: x sweeps then y sweeps, LPC = NT/32 lines per chunk.
 // ---------------------------------------------------------------------------
@@ -746,6 +772,7 @@ struct DevCtx {
         return v;
     }
     __device__ __forceinline__ bool warp_any(bool p) const { return __any_sync(0xffffffffu, p) != 0; }
+    __device__ __forceinline__ void prefetch_l2(const void* p) const { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
 };
 #endif
 
