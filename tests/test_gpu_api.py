@@ -200,6 +200,36 @@ def test_config2_full_size_first_steps(orc):
     assert np.array_equal(sol.state.q, ref.q)
 
 
+def test_config2_full_size_full_run(orc):
+    """The benchmark workload itself: 1280x320 shock bubble run to t = 0.6
+    (about 3000 controlled steps) by the device loop equals the oracle's C
+    replay of evolve_to_time cell for cell (the bar is 1e-11 relative per
+    cell), with the same number of steps and the same final time."""
+    import ctypes
+    import bench
+    from pyclaw_b200 import _abi, _lib
+    from pyclaw_b200.device import DeviceState
+    p, q, aux, run, tfinal = bench.shockbubble_config()
+    dev = DeviceState(p)
+    dev.upload_q(q)
+    c = _abi.Control()
+    _lib.load().claw2_control_init(ctypes.byref(c), 0.0, run['dt_initial'], tfinal, run['cfl_max'],
+                                   run['cfl_desired'], 1e99, 1, 0, 100000, run['cfl_desired'])
+    out = dev.evolve(c)
+    got = dev.download_q()
+    assert out.error == 0 and abs(out.t - tfinal) == 0.0
+    qbc = orc.new_qbc(p, q)
+    ctrl = orc.control_init(0.0, run['dt_initial'], tfinal, run['cfl_max'], run['cfl_desired'], max_steps=100000)
+    rc = orc.evolve(p, qbc, None, ctrl, omp=True)
+    assert rc == 0, rc
+    ref = np.array(qbc[:, 2:-2, 2:-2])
+    for m in range(4):
+        rel = np.max(np.abs(got[m] - ref[m])) / np.max(np.abs(ref[m]))
+        assert rel <= 1e-11, (m, rel)
+    assert np.array_equal(got, ref)
+    assert out.numsteps == ctrl.numsteps and out.t == ctrl.t and out.rejected == ctrl.rejected
+
+
 def test_walled_euler_conserves_mass_and_energy():
     import bench
     p, q, aux, run, tfinal = bench.shockbubble_config(320, 80, walls=True)
