@@ -31,6 +31,10 @@ CASES += [
     ("euler5", 3, 2, 2, 2, (1, 1), (1, 1)),        # tiny grid: separate ghost fill
     ("euler4", 300, 7, 2, 2, (1, 3), (1, 3)),      # long and thin
     ("euler4", 7, 300, -1, 2, (1, 3), (1, 3)),
+    # grids of at least 148 29x29 tiles: the acoustics bodies' large-tile form
+    # (smaller grids run 13x13 tiles)
+    ("vc_acoustics", 400, 380, 2, 2, (1, 3), (3, 1)),
+    ("acoustics", 420, 360, 1, 2, (3, 2), (3, 2)),
 ]
 
 
