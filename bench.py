@@ -225,7 +225,10 @@ class ClockSampler(object):
     def __init__(self, gpu_index):
         self.idx = gpu_index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", "clocks_bench_%d.csv" % gpu_index)
+        # the raw samples go to $CLAW2_CLOCKS_DIR (default: the system temp dir)
+        import tempfile
+        d = os.environ.get("CLAW2_CLOCKS_DIR") or tempfile.gettempdir()
+        self.path = os.path.join(d, "clocks_bench_%d_%d.csv" % (gpu_index, os.getpid()))
 
     def start(self):
         try:
