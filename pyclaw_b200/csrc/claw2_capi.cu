@@ -72,6 +72,8 @@ template <> struct HasLean<RpShallow> { static constexpr bool value = true; };
 #ifndef CLAW2_LEAN_MINB
 #define CLAW2_LEAN_MINB 2
 #endif
+// lean tiles: 28 x 28 cells, so that a line's 32 lanes hold its 32 cells
+constexpr int LTX = 28, LTY = 28;
 
 template <class RP>
 __global__ void __launch_bounds__(256, CLAW2_LEAN_MINB) lean_step_kernel(StepArgs a)
@@ -80,7 +82,7 @@ __global__ void __launch_bounds__(256, CLAW2_LEAN_MINB) lean_step_kernel(StepArg
     DevCtx ctx{smem_dyn};
     const TileId t{(int)blockIdx.x, (int)blockIdx.y, (int)gridDim.x, (int)gridDim.y,
                    (int)(blockIdx.y * gridDim.x + blockIdx.x), (int)(gridDim.x * gridDim.y)};
-    lean_tile_at<RP, 29, 29, 256>(a, ctx, t);
+    lean_tile_at<RP, LTX, LTY, 256>(a, ctx, t);
 }
 
 // Instance of tile t: the last one with tile_begin <= t (binary search).
@@ -324,6 +326,11 @@ void tiles(const claw2_problem* p, int* nbx, int* nby)
     const bool light = !split && p->index_capa < 0 && !p->use_fwave &&
                        (p->rp == CLAW2_RP_ACOUSTICS || p->rp == CLAW2_RP_VC_ACOUSTICS);
     if (light && light_small_grid(p->mx, p->my)) tx = ty = LIGHT_SMALL_TILE;
+    // the lean body's tiles (launch_step_t)
+    const bool lean = !split && p->index_capa < 0 && !p->use_fwave &&
+                      (p->rp == CLAW2_RP_EULER_4WAVE || p->rp == CLAW2_RP_EULER_5WAVE ||
+                       p->rp == CLAW2_RP_SHALLOW_ROE);
+    if (lean) { tx = LTX; ty = LTY; }
     *nbx = (p->mx + tx - 1) / tx;
     *nby = (p->my + ty - 1) / ty;
 }
@@ -374,7 +381,7 @@ int launch_light(const StepArgs& a, int nbx, int nby, cudaStream_t st)
 template <class RP>
 int launch_lean(const StepArgs& a, int nbx, int nby, cudaStream_t st)
 {
-    using SM = LeanSmem<RP, 29, 29, 256>;
+    using SM = LeanSmem<RP, LTX, LTY, 256>;
     auto kern = lean_step_kernel<RP>;
     static bool configured = false;
     if (!configured) {

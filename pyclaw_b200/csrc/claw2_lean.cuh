@@ -4,6 +4,12 @@
 // Same step as step_tile_at (step2.f90:92-248 / flux2.f90:104-206) with the
 // same operations in the same order, so the results are the same values; only
 // the data movement differs, as in the acoustics body of claw2_light.cuh:
+//  - each lane computes the quantities of one cell that the normal solve
+//    needs (RP::Cell: square roots, pressures, Roe-average numerators) and
+//    takes those of the cell right of its interface from the next lane, so
+//    each cell's are computed once per line instead of once per interface;
+//    with TX = 28 the 32 lanes hold the 32 cells i0-2 .. i0+29 of the line's
+//    31 interfaces;
 //  - the normal solve stays in registers; for the limiter each lane takes its
 //    right neighbour's wave by warp shuffle and forms dotr = wave(k).wave(k+1);
 //    dotl of lane k is dotr of lane k-1 (one more shuffle), the same products
@@ -31,8 +37,7 @@ template <class RP, int TX, int TY, int NT> struct LeanSmem {
     static constexpr int QX = MEQN * TX * TY;
     static constexpr int CX = 2 * 2 * MEQN * NT;
     static constexpr int TR = TY + 4;            // rows j0-2 .. j0+TY+1
-    static constexpr int TP = TX + 4;            // columns i0-2 .. i0+TX+1
-    static_assert(TP % 2 == 1, "the halo pitch must be odd");
+    static constexpr int TP = (TX + 4) | 1;      // columns i0-2 .. i0+TX+1, odd pitch
     static constexpr int HS = MEQN * TR * TP;
     static constexpr int total = QX + CX + NT + HS;
     static constexpr int bytes = total * 8;
@@ -93,15 +98,21 @@ CLAW2_HD void lean_chunk(const StepArgs& a, Ctx& ctx, const double* H, double* Q
     for (int m = 0; m < MEQN; m++) { amdq[m] = 0.0; apdq[m] = 0.0; }
 #pragma unroll
     for (int r = 0; r < NROE; r++) roe[r] = 0.0;
-    if (ifok) {
-        double qL[MEQN], qR[MEQN];
+    {
+        // this lane's cell k-1, and cell k from the next lane
+        typename RP::Cell L{};
+        double qL[MEQN];
+        const bool cellok = lineok && k - 1 <= len + 1;
 #pragma unroll
-        for (int m = 0; m < MEQN; m++) {
-            qL[m] = hq(m, k - 1, line);
-            qR[m] = hq(m, k, line);
+        for (int m = 0; m < MEQN; m++) qL[m] = cellok ? hq(m, k - 1, line) : 0.0;
+        if (cellok) L = RP::template cell<IXY>(qL, a.prm);
+        const typename RP::Cell R = L.map([&](double v) { return ctx.shfl_down(v); });
+        if (ifok) {
+            double qR[MEQN];
+#pragma unroll
+            for (int m = 0; m < MEQN; m++) qR[m] = hq(m, k, line);
+            RP::template rpn2c<IXY>(qL, qR, L, R, a.prm, wave, s, amdq, apdq, roe);
         }
-        const double noaux[1] = {0.0};
-        RP::template rpn2<IXY>(qL, qR, noaux, noaux, a.prm, wave, s, amdq, apdq, roe);
     }
 
     // ---------------- CFL, limiter, second-order corrections ----------------

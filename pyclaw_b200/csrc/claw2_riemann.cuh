@@ -42,24 +42,57 @@ template <bool TRACER> struct RpEuler {
     static constexpr int MAUX = 0;
     static constexpr int NROE = 7;   // u, v, a, enth, u2v2, g1a2, euv
 
+    // What rpn2 computes from one cell alone, for either of the cell's two
+    // interfaces along a slice: sqrt(rho), the pressure, the three Roe-average
+    // numerators (rhou/sqrt(rho), rhov/sqrt(rho), (E+p)/sqrt(rho)) and, for the
+    // entropy fix, the normal velocity rhou/rho and the sound speed
+    // sqrt(gamma*p/rho).  The lean tile body computes them once per cell and
+    // hands them to the neighbouring interface by warp shuffle.
+    struct Cell {
+        double sq, p, U, V, H, un, c;
+        template <class F> CLAW2_DEV Cell map(F f) const { return Cell{f(sq), f(p), f(U), f(V), f(H), f(un), f(c)}; }
+    };
+    template <int IXY>
+    static CLAW2_DEV Cell cell(const double (&q)[MEQN], const double* prm)
+    {
+        constexpr int mu = Dir<IXY>::MU, mv = Dir<IXY>::MV;
+        const double gamma = prm[0], gamma1 = prm[1];
+        Cell c;
+        c.sq = sqrt(q[0]);
+        c.p = gamma1 * (q[3] - 0.5 * (q[1] * q[1] + q[2] * q[2]) / q[0]);
+        c.U = q[mu] / c.sq;
+        c.V = q[mv] / c.sq;
+        c.H = (q[3] + c.p) / c.sq;
+        c.un = q[mu] / q[0];
+        c.c = sqrt(gamma * c.p / q[0]);
+        return c;
+    }
+
     template <int IXY>
     static CLAW2_DEV void rpn2(const double (&qL)[MEQN], const double (&qR)[MEQN],
-                                                const double*, const double*, const double* prm,
+                                                const double* auxL, const double* auxR, const double* prm,
                                                 double (&wave)[MW][MEQN], double (&s)[MW],
                                                 double (&amdq)[MEQN], double (&apdq)[MEQN],
                                                 double (&roe)[NROE])
     {
+        rpn2c<IXY>(qL, qR, cell<IXY>(qL, prm), cell<IXY>(qR, prm), prm, wave, s, amdq, apdq, roe);
+    }
+
+    // rpn2 with the two cells' quantities given (Cell, same expressions)
+    template <int IXY>
+    static CLAW2_DEV void rpn2c(const double (&qL)[MEQN], const double (&qR)[MEQN], const Cell& L, const Cell& R,
+                                const double* prm, double (&wave)[MW][MEQN], double (&s)[MW],
+                                double (&amdq)[MEQN], double (&apdq)[MEQN], double (&roe)[NROE])
+    {
         constexpr int mu = Dir<IXY>::MU, mv = Dir<IXY>::MV;
         const double gamma = prm[0], gamma1 = prm[1];
-        // Roe averages, :87-104
-        const double rhsqrtl = sqrt(qL[0]);
-        const double rhsqrtr = sqrt(qR[0]);
-        const double pl = gamma1 * (qL[3] - 0.5 * (qL[1] * qL[1] + qL[2] * qL[2]) / qL[0]);
-        const double pr = gamma1 * (qR[3] - 0.5 * (qR[1] * qR[1] + qR[2] * qR[2]) / qR[0]);
+        // Roe averages, :87-104: u = (qL(mu)/sqrt(rhoL) + qR(mu)/sqrt(rhoR))/(sqrt(rhoL)+sqrt(rhoR)), ...
+        const double rhsqrtl = L.sq;
+        const double rhsqrtr = R.sq;
         const double rhsq2 = rhsqrtl + rhsqrtr;
-        const double u = (qL[mu] / rhsqrtl + qR[mu] / rhsqrtr) / rhsq2;
-        const double v = (qL[mv] / rhsqrtl + qR[mv] / rhsqrtr) / rhsq2;
-        const double enth = ((qL[3] + pl) / rhsqrtl + (qR[3] + pr) / rhsqrtr) / rhsq2;
+        const double u = (L.U + R.U) / rhsq2;
+        const double v = (L.V + R.V) / rhsq2;
+        const double enth = (L.H + R.H) / rhsq2;
         const double u2v2 = u * u + v * v;
         const double asq = gamma1 * (enth - .5 * u2v2);
         const double a = sqrt(asq);
@@ -93,12 +126,11 @@ template <bool TRACER> struct RpEuler {
 
         // entropy fix, :205-286
         {
-            const double rhoim1 = qL[0];
-            // gamma1*(qr(4,i-1) - 0.5*(qr(mu,i-1)**2 + qr(mv,i-1)**2)/rhoim1) is pl bit for bit:
-            // the two squares are the same and IEEE addition commutes
-            const double pim1 = pl;
-            const double cim1 = sqrt(gamma * pim1 / rhoim1);
-            const double s0 = qL[mu] / rhoim1 - cim1;
+            // cim1 = sqrt(gamma*pim1/rhoim1) and qr(mu,i-1)/rhoim1 of the left cell;
+            // gamma1*(qr(4,i-1) - 0.5*(qr(mu,i-1)**2 + qr(mv,i-1)**2)/rhoim1) is its
+            // pressure bit for bit: the two squares are the same and IEEE addition commutes
+            const double cim1 = L.c;
+            const double s0 = L.un - cim1;
             if (s0 >= 0.0 && s[0] > 0.0) {
 #pragma unroll
                 for (int m = 0; m < MEQN; m++) amdq[m] = 0.0;
@@ -126,10 +158,8 @@ template <bool TRACER> struct RpEuler {
                     amdq[3] = amdq[3] + s[1] * wave[1][3];
                     amdq[3] = amdq[3] + s[2] * wave[2][3];
                     if constexpr (TRACER) amdq[4] = amdq[4] + s[4] * wave[4][4];
-                    const double rhoi = qR[0];
-                    const double pi = pr;   // same value as pr, see pim1
-                    const double ci = sqrt(gamma * pi / rhoi);
-                    const double s3 = qR[mu] / rhoi + ci;
+                    const double ci = R.c;              // the right cell's, as cim1
+                    const double s3 = R.un + ci;
                     const double rho2 = qR[0] - wave[3][0];
                     const double rhou2 = qR[mu] - wave[3][mu];
                     const double rhov2 = qR[mv] - wave[3][mv];
@@ -300,6 +330,27 @@ struct RpVcAcoustics {
 struct RpShallow {
     static constexpr int MEQN = 3, MW = 3, MAUX = 0, NROE = 3;   // ubar, vbar, cbar
 
+    // What rpn2 computes from one cell alone (see RpEuler::Cell): sqrt(h),
+    // the Roe-average numerators hu/sqrt(h), hv/sqrt(h), and for the
+    // transonic fix the normal velocity hu/h and the wave speed sqrt(g h).
+    struct Cell {
+        double sq, U, V, un, c;
+        template <class F> CLAW2_DEV Cell map(F f) const { return Cell{f(sq), f(U), f(V), f(un), f(c)}; }
+    };
+    template <int IXY>
+    static CLAW2_DEV Cell cell(const double (&q)[MEQN], const double* prm)
+    {
+        constexpr int mu = Dir<IXY>::MU, mv = Dir<IXY>::MV;
+        const double grav = prm[0];
+        Cell c;
+        c.sq = sqrt(q[0]);
+        c.U = q[mu] / c.sq;
+        c.V = q[mv] / c.sq;
+        c.un = q[mu] / q[0];
+        c.c = sqrt(grav * q[0]);
+        return c;
+    }
+
     template <int IXY>
     static CLAW2_DEV void rpn2(const double (&qL)[MEQN], const double (&qR)[MEQN],
                                                 const double*, const double*, const double* prm,
@@ -307,13 +358,22 @@ struct RpShallow {
                                                 double (&amdq)[MEQN], double (&apdq)[MEQN],
                                                 double (&roe)[NROE])
     {
+        rpn2c<IXY>(qL, qR, cell<IXY>(qL, prm), cell<IXY>(qR, prm), prm, wave, s, amdq, apdq, roe);
+    }
+
+    // rpn2 with the two cells' quantities given (Cell, same expressions)
+    template <int IXY>
+    static CLAW2_DEV void rpn2c(const double (&qL)[MEQN], const double (&qR)[MEQN], const Cell& L, const Cell& R,
+                                const double* prm, double (&wave)[MW][MEQN], double (&s)[MW],
+                                double (&amdq)[MEQN], double (&apdq)[MEQN], double (&roe)[NROE])
+    {
         constexpr int mu = Dir<IXY>::MU, mv = Dir<IXY>::MV;
         const double grav = prm[0];
         const double hl = qL[0], hr = qR[0];
-        const double hsqrtl = sqrt(hl), hsqrtr = sqrt(hr);
+        const double hsqrtl = L.sq, hsqrtr = R.sq;
         const double hsq2 = hsqrtl + hsqrtr;
-        const double ubar = (qL[mu] / hsqrtl + qR[mu] / hsqrtr) / hsq2;
-        const double vbar = (qL[mv] / hsqrtl + qR[mv] / hsqrtr) / hsq2;
+        const double ubar = (L.U + R.U) / hsq2;
+        const double vbar = (L.V + R.V) / hsq2;
         const double hbar = 0.5 * (hl + hr);
         const double cbar = sqrt(grav * hbar);
         const double delta1 = hr - hl;
@@ -327,7 +387,7 @@ struct RpShallow {
         wave[1][0] = 0.0; wave[1][mu] = 0.0; wave[1][mv] = a2; s[1] = ubar;
         wave[2][0] = a3; wave[2][mu] = a3 * (ubar + cbar); wave[2][mv] = a3 * vbar; s[2] = ubar + cbar;
 
-        const double s0 = qL[mu] / hl - sqrt(grav * hl);
+        const double s0 = L.un - L.c;          // qL(mu)/hl - sqrt(grav*hl)
         if (s0 >= 0.0 && s[0] > 0.0) {
             amdq[0] = 0.0; amdq[1] = 0.0; amdq[2] = 0.0;
         } else {
@@ -342,7 +402,7 @@ struct RpShallow {
             for (int m = 0; m < MEQN; m++) amdq[m] = sfract * wave[0][m];
             if (s[1] < 0.0) {
                 amdq[mv] = amdq[mv] + s[1] * wave[1][mv];
-                const double s3 = qR[mu] / hr + sqrt(grav * hr);
+                const double s3 = R.un + R.c;  // qR(mu)/hr + sqrt(grav*hr)
                 const double h2 = hr - wave[2][0];
                 const double hu2 = qR[mu] - wave[2][mu];
                 const double s2 = hu2 / h2 + sqrt(grav * h2);
