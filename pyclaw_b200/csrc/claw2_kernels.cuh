@@ -578,7 +578,8 @@ CLAW2_HD void euler_radial_source(double (&v)[MEQN], double rad, double gamma1, 
     }
 }
 
-template <int MEQN, int TX, int TY, int NT, class Ctx>
+// QP: row pitch of Qx in doubles (TX unless the body pads its rows)
+template <int MEQN, int TX, int TY, int NT, int QP = TX, class Ctx>
 CLAW2_HD void finish_tile(const StepArgs& a, Ctx& ctx, const TileId& tile, const double* Qx, int QSTR, double* red,
                           double* qout, int i0, int j0, double cflm, double dt)
 {
@@ -590,7 +591,7 @@ CLAW2_HD void finish_tile(const StepArgs& a, Ctx& ctx, const TileId& tile, const
         if (i >= a.mx || j >= a.my) continue;
         double v[MEQN];
 #pragma unroll
-        for (int m = 0; m < MEQN; m++) v[m] = Qx[m * QSTR + cj * TX + ci];
+        for (int m = 0; m < MEQN; m++) v[m] = Qx[m * QSTR + cj * QP + ci];
         if (a.src == CLAW2_SRC_EULER_RADIAL)
             euler_radial_source<MEQN>(v, a.aux[qoff(a, a.src_aux, i, j)], a.prm[1], dt);
 #pragma unroll

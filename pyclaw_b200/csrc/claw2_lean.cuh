@@ -34,7 +34,9 @@ namespace claw2 {
 // staged input halo (MEQN fields x TR rows x TP columns).
 template <class RP, int TX, int TY, int NT> struct LeanSmem {
     static constexpr int MEQN = RP::MEQN;
-    static constexpr int QX = MEQN * TX * TY;
+    static constexpr int QP = TX | 1;            // row pitch of the tile state: odd, so that
+                                                 // y lines walking down a column avoid bank conflicts
+    static constexpr int QX = MEQN * TY * QP;
     static constexpr int CX = 2 * 2 * MEQN * NT;
     static constexpr int TR = TY + 4;            // rows j0-2 .. j0+TY+1
     static constexpr int TP = (TX + 4) | 1;      // columns i0-2 .. i0+TX+1, odd pitch
@@ -221,7 +223,7 @@ CLAW2_HD void lean_chunk(const StepArgs& a, Ctx& ctx, const double* H, double* Q
     if (cellok) {
         auto qx = [&](int m, int kk, int ll) -> double& {
             const int ci = IXY == 1 ? kk : ll, cj = IXY == 1 ? ll : kk;
-            return Qx[(m * TY + (cj - j0)) * TX + (ci - i0)];
+            return Qx[(m * TY + (cj - j0)) * SM::QP + (ci - i0)];
         };
         auto qi = [&](int m, int kk, int ll) -> double { return IXY == 1 ? hq(m, kk, ll) : qx(m, kk, ll); };
         auto in_tile_line = [&](int ll) {
@@ -315,7 +317,7 @@ CLAW2_HD void lean_tile_at(const StepArgs& a, Ctx& ctx, const TileId& tile)
         }
     }
     ctx.sync();
-    finish_tile<MEQN, TX, TY, NT>(a, ctx, tile, Qx, TX * TY, red, qout, i0, j0, cflm, dt);
+    finish_tile<MEQN, TX, TY, NT, SM::QP>(a, ctx, tile, Qx, TY * SM::QP, red, qout, i0, j0, cflm, dt);
 }
 
 }  // namespace claw2
