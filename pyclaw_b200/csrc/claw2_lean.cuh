@@ -272,7 +272,7 @@ CLAW2_HD void lean_tile_at(const StepArgs& a, Ctx& ctx, const TileId& tile)
     constexpr int MEQN = RP::MEQN;
     using SM = LeanSmem<RP, TX, TY, NT>;
     constexpr int LPC = NT / 32;
-    static_assert(TX + 3 <= 32 && TY + 3 <= 32, "tile too wide for one 32-lane line");
+    static_assert(TX + 4 <= 32 && TY + 4 <= 32, "a line's cells i0-2 .. i0+TX+1 must fit its 32 lanes");
     static_assert(RP::MAUX == 0, "the lean body serves the solvers without aux arrays");
     double* Qx = ctx.smem();
     double* CX = Qx + SM::QX;
