@@ -103,12 +103,14 @@ __device__ __forceinline__ int batch_instance_of(const claw2_batch_instance* __r
 // once per step, from HBM, so the tile's first loads would otherwise wait for
 // DRAM.  One prefetch per 128-byte line, spread over the CTA's threads.  The
 // addresses stay inside the instance's arrays; results do not depend on it.
+// Returns tile t's instance.
 template <int MEQN, int MAUX, int TX, int TY, int NT>
-__device__ __forceinline__ void batch_prefetch_tile(const claw2_batch_instance* __restrict__ inst, int ninst, int t)
+__device__ __forceinline__ int batch_prefetch_tile(const claw2_batch_instance* __restrict__ inst, int ninst, int t)
 {
-    const claw2_batch_instance& I = inst[batch_instance_of(inst, ninst, t)];
+    const int k = batch_instance_of(inst, ninst, t);
+    const claw2_batch_instance& I = inst[k];
     const claw2_control* c = I.ctrl;
-    if (c->done) return;
+    if (c->done) return k;
     const double* q = c->cur ? I.q1 : I.q0;
     const int lt = t - I.tile_begin;
     const int i0 = (lt % I.nbx) * TX, j0 = (lt / I.nbx) * TY;
@@ -126,6 +128,7 @@ __device__ __forceinline__ void batch_prefetch_tile(const claw2_batch_instance* 
         const char* ptr = base + (long long)(rlo + r + CLAW2_NUM_GHOST) * I.ld * 8 + ((long long)(l0 + line) << 7);
         asm volatile("prefetch.global.L2 [%0];" ::"l"(ptr));
     }
+    return k;
 }
 
 // Batched step: a persistent grid walks the concatenated tile list of all
@@ -137,10 +140,12 @@ batch_kernel(const claw2_batch_instance* __restrict__ inst, int ninst, int ntile
 {
     extern __shared__ double smem_dyn[];
     DevCtx ctx{smem_dyn};
+    int next = -1;                                  // instance of the next tile, found by its prefetch
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-        if (t + (int)gridDim.x < ntiles)
-            batch_prefetch_tile<RP::MEQN, RP::MAUX, 29, 29, NT>(inst, ninst, t + (int)gridDim.x);
-        const int lo = batch_instance_of(inst, ninst, t);
+        const int lo = next >= 0 ? next : batch_instance_of(inst, ninst, t);
+        next = t + (int)gridDim.x < ntiles
+                   ? batch_prefetch_tile<RP::MEQN, RP::MAUX, 29, 29, NT>(inst, ninst, t + (int)gridDim.x)
+                   : -1;
         const claw2_batch_instance& I = inst[lo];
         StepArgs a = common;
         a.q0 = I.q0; a.q1 = I.q1; a.aux = I.aux; a.ctrl = I.ctrl;
