@@ -120,13 +120,12 @@ __device__ __forceinline__ int batch_prefetch_tile(const claw2_batch_instance* _
     const long long b0 = (long long)(clo + CLAW2_NUM_GHOST) * 8, b1 = (long long)(chi + CLAW2_NUM_GHOST) * 8 + 8;
     const int l0 = (int)(b0 >> 7), nl = (int)((b1 + 127) >> 7) - l0;
     const int nrow = rhi - rlo + 1;
-    const int items = (MEQN + MAUX) * nrow * nl;
-    for (int k = threadIdx.x; k < items; k += NT) {
-        const int line = k % nl, rf = k / nl;
+    // one (field, row) per thread, its 128-byte lines in turn
+    for (int rf = threadIdx.x; rf < (MEQN + MAUX) * nrow; rf += NT) {
         const int r = rf % nrow, f = rf / nrow;
         const char* base = f < MEQN ? (const char*)(q + f * I.plane) : (const char*)(I.aux + (f - MEQN) * I.plane);
-        const char* ptr = base + (long long)(rlo + r + CLAW2_NUM_GHOST) * I.ld * 8 + ((long long)(l0 + line) << 7);
-        asm volatile("prefetch.global.L2 [%0];" ::"l"(ptr));
+        const char* row = base + (long long)(rlo + r + CLAW2_NUM_GHOST) * I.ld * 8 + ((long long)l0 << 7);
+        for (int line = 0; line < nl; line++) asm volatile("prefetch.global.L2 [%0];" ::"l"(row + (line << 7)));
     }
     return k;
 }

@@ -525,12 +525,12 @@ CLAW2_HD void prefetch_box(Ctx& ctx, const double* base, int nf, long long P, lo
     const long long b0 = (long long)(c0 + CLAW2_NUM_GHOST) * 8, b1 = (long long)(c1 + CLAW2_NUM_GHOST) * 8 + 8;
     const int l0 = (int)(b0 >> 7), nl = (int)((b1 + 127) >> 7) - l0;
     const int nrow = r1 - r0 + 1;
-    const int items = nf * nrow * nl;
-    for (int k = ctx.tid(); k < items; k += NT) {
-        const int line = k % nl, rf = k / nl;
+    // one (field, row) per thread, its 128-byte lines in turn
+    for (int rf = ctx.tid(); rf < nf * nrow; rf += NT) {
         const int r = rf % nrow, f = rf / nrow;
-        ctx.prefetch_l2((const char*)(base + f * P) + (long long)(r0 + r + CLAW2_NUM_GHOST) * ld * 8 +
-                        ((long long)(l0 + line) << 7));
+        const char* row = (const char*)(base + f * P) + (long long)(r0 + r + CLAW2_NUM_GHOST) * ld * 8 +
+                          ((long long)l0 << 7);
+        for (int line = 0; line < nl; line++) ctx.prefetch_l2(row + (line << 7));
     }
 }
 
