@@ -51,7 +51,7 @@ def _centers(lower, upper, n):
     return c, delta
 
 
-def shockbubble_config(mx=1280, my=320, walls=False):
+def shockbubble_config(mx=1280, my=320, walls=False, split=False):
     """Returns (problem, q0, aux0, run_kwargs, tfinal) for the shock-bubble workload."""
     from pyclaw_b200 import _abi
     x, dx = _centers(0.0, 2.0, mx)
@@ -75,7 +75,7 @@ def shockbubble_config(mx=1280, my=320, walls=False):
     q[3] = p / gamma1 + 0.5 * rho * u * u
     bcx = _abi.BC_WALL if walls else _abi.BC_EXTRAP
     prob = _abi.make_problem(rp=_abi.RP_EULER_4WAVE, num_eqn=4, num_waves=4, num_aux=0, mx=mx, my=my,
-                             dx=dx, dy=dy, order=2, transverse=2, mthlim=[4],
+                             dx=dx, dy=dy, order=2, transverse=-1 if split else 2, mthlim=[4],
                              bc_lower=(bcx, _abi.BC_WALL), bc_upper=(bcx, _abi.BC_WALL),
                              params=(GAMMA, gamma1))
     smax = abs(u2) + np.sqrt(GAMMA * p2 / rho2)
@@ -347,7 +347,7 @@ def run_reference_arm(args, world, rank):
     """--impl reference: the oracle (OpenMP gather form, all host threads)."""
     if rank != 0:
         return
-    prob, q, aux, run, tfinal = shockbubble_config()
+    prob, q, aux, run, tfinal = shockbubble_config(split=args.split)
     from oracle import oracle as O
     lib = O.load(True)
     qbc = O.new_qbc(prob, q)
@@ -378,7 +378,8 @@ def run_reference_arm(args, world, rank):
         "ms_per_step": el / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": "euler_shockbubble_1280x320", "mx": prob.mx, "my": prob.my,
-                   "solver": "euler_roe_efix_4wave", "limiter": "MC", "transverse_waves": 2},
+                   "solver": "euler_roe_efix_4wave", "limiter": "MC", "transverse_waves": -1 if args.split else 2,
+                       "mode": "dimensional splitting" if args.split else "unsplit"},
         "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": threads, "kind": "port",
                          "sample": "%d whole-grid steps (BC fill + step + dt control) of the 1280x320 "
                                    "shock bubble, oracle OpenMP gather form, %d threads" % (args.steps, threads)},
@@ -397,7 +398,7 @@ def run_ours(args, world, rank, local):
     from pyclaw_b200.device import DeviceState
 
     lib = _lib.load()
-    prob, q, aux, run, tfinal = shockbubble_config()
+    prob, q, aux, run, tfinal = shockbubble_config(split=args.split)
     cells = prob.mx * prob.my
     c = _abi.Control()
     _lib.check(lib.claw2_control_init(ctypes.byref(c), 0.0, run['dt_initial'], 1e9, run['cfl_max'],
@@ -475,7 +476,8 @@ def run_ours(args, world, rank, local):
     avg_kernel_s = t_dev / args.steps
     achieved = alg_bytes / avg_kernel_s / 1e9
     traffic = None
-    tpath = os.path.join(ROOT, "profiles", "lean_step_kernel_euler1280x320.md")
+    tpath = os.path.join(ROOT, "profiles", "step_kernel_split_euler1280x320.md" if args.split
+                         else "lean_step_kernel_euler1280x320.md")
     if os.path.exists(tpath):            # dram read+write bytes of one launch, from the ncu capture
         with open(tpath) as f:
             for ln in f:
@@ -505,7 +507,8 @@ def run_ours(args, world, rank, local):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
             "config": {"workload": "euler_shockbubble_1280x320", "mx": prob.mx, "my": prob.my,
-                       "solver": "euler_roe_efix_4wave", "limiter": "MC", "transverse_waves": 2,
+                       "solver": "euler_roe_efix_4wave", "limiter": "MC", "transverse_waves": -1 if args.split else 2,
+                       "mode": "dimensional splitting" if args.split else "unsplit",
                        "parallelism": ("domain decomposition: %d slabs of 1280x320 along y of one 1280x%d grid, "
                                        "NCCL halo exchange + CFL max all-reduce per step" % (world, 320 * world))
                        if world > 1 else "single",
@@ -879,6 +882,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--split", action="store_true",
+                    help="shock bubble with dimensional splitting (the reference's default mode)")
     ap.add_argument("--workload", default="shockbubble", choices=["shockbubble", "batched", "adjoint", "shallow", "acoustics"])
     ap.add_argument("--sw-n", type=int, default=4096)
     ap.add_argument("--sw-steps", type=int, default=500)
