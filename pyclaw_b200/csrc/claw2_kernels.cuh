@@ -202,7 +202,8 @@ template <class RP, int TX, int TY, int NT, bool SPLIT> struct TileSmem {
     static constexpr int QROWS = SPLIT ? TY + 4 : TY;
     static constexpr int WBSZ = CMax<MW * MEQN + MW, 5 * MEQN>::value;
     static constexpr int B2SZ = CMax<2 * MEQN + NROE, 4 * MEQN>::value;
-    static constexpr int QX = MEQN * QROWS * TX;
+    static constexpr int QP = TX | 1;    // row pitch of Qx: odd, so that y lines down a column avoid bank conflicts
+    static constexpr int QX = MEQN * QROWS * QP;
     static constexpr int total = QX + (WBSZ + B2SZ) * NT + NT;      // + reduction scratch
     static constexpr int bytes = total * 8;
 };
@@ -228,6 +229,7 @@ CLAW2_HD void sweep_chunk(const StepArgs& a, Ctx& ctx, const double* qin, double
 {
     constexpr int MEQN = RP::MEQN, MW = RP::MW, MAUX = RP::MAUX, NROE = RP::NROE;
     constexpr int QROWS = SPLIT ? TY + 4 : TY;
+    constexpr int QP = TX | 1;                 // row pitch of Qx (TileSmem::QP)
     constexpr int QROW0 = SPLIT ? -2 : 0;      // tile row of Qx row 0, relative to j0
     constexpr int AUXN = MAUX > 0 ? MAUX : 1;
     constexpr int NCELL = IXY == 1 ? TX : TY;  // cells of the tile along the slice
@@ -260,8 +262,8 @@ CLAW2_HD void sweep_chunk(const StepArgs& a, Ctx& ctx, const double* qin, double
             // y sweep of the split step reads the x-swept tile state
 #pragma unroll
             for (int m = 0; m < MEQN; m++) {
-                qL[m] = Qx[(m * QROWS + (jL - j0 - QROW0)) * TX + (iL - i0)];
-                qR[m] = Qx[(m * QROWS + (jR - j0 - QROW0)) * TX + (iR - i0)];
+                qL[m] = Qx[(m * QROWS + (jL - j0 - QROW0)) * QP + (iL - i0)];
+                qR[m] = Qx[(m * QROWS + (jR - j0 - QROW0)) * QP + (iR - i0)];
             }
         } else {
 #pragma unroll
@@ -401,7 +403,7 @@ CLAW2_HD void sweep_chunk(const StepArgs& a, Ctx& ctx, const double* qin, double
     const bool trans = !SPLIT && a.trans > 0;
     auto qx = [&](int m, int kk, int ll) -> double& {
         const int ci = IXY == 1 ? kk : ll, cj = IXY == 1 ? ll : kk;
-        return Qx[(m * QROWS + (cj - j0 - QROW0)) * TX + (ci - i0)];
+        return Qx[(m * QROWS + (cj - j0 - QROW0)) * QP + (ci - i0)];
     };
     auto capa_of = [&](int kk, int ll) {
         return a.aux[qoff(a, a.capa, IXY == 1 ? kk : ll, IXY == 1 ? ll : kk)];
@@ -731,7 +733,8 @@ CLAW2_HD void step_tile_at(const StepArgs& a, Ctx& ctx, const TileId& tile)
         }
     }
 
-    finish_tile<MEQN, TX, TY, NT>(a, ctx, tile, Qx + (-QROW0) * TX, QROWS * TX, red, qout, i0, j0, cflm, dt);
+    finish_tile<MEQN, TX, TY, NT, SM::QP>(a, ctx, tile, Qx + (-QROW0) * SM::QP, QROWS * SM::QP, red, qout, i0, j0,
+                                         cflm, dt);
 }
 
 template <class RP, int TX, int TY, int NT, bool SPLIT, class Ctx>
