@@ -61,6 +61,12 @@ struct StepArgs {
 
 template <int IXY> struct Phase;
 
+// Solvers whose rpn2 splits into per-cell quantities (RP::Cell, RP::cell,
+// RP::rpn2c): the Euler and shallow-water Roe solvers.
+template <class RP> struct HasCell { static constexpr bool value = false; };
+template <bool T> struct HasCell<RpEuler<T>> { static constexpr bool value = true; };
+template <> struct HasCell<RpShallow> { static constexpr bool value = true; };
+
 CLAW2_HD long long qoff(const StepArgs& a, int m, int i, int j)
 {
     return (long long)m * a.plane + (long long)(j + CLAW2_NUM_GHOST) * a.ld + (i + CLAW2_NUM_GHOST);
@@ -252,32 +258,24 @@ CLAW2_HD void sweep_chunk(const StepArgs& a, Ctx& ctx, const double* qin, double
 
     double dtl = dtn, dtr = dtn;
     // ---------------- S1: normal Riemann solve ----------------
-    if (ifok) {
-        double qL[MEQN], qR[MEQN], auxL[AUXN], auxR[AUXN];
-        double wave[MW][MEQN], s[MW], amdq[MEQN], apdq[MEQN], roe[NROE];
-        const int iL = cell_i(k - 1), jL = cell_j(k - 1), iR = cell_i(k), jR = cell_j(k);
-        const long long oL = qoff(a, 0, iL, jL);
-        const long long oR = oL + (IXY == 1 ? 1 : a.ld);      // cell k: one step along the slice
-        if (SPLIT && IXY == 2 && !cflonly) {
-            // y sweep of the split step reads the x-swept tile state
+    // A line's 32 lanes hold its cells k-1 = i0-2 .. when NCELL + 4 <= 32: then
+    // the solvers with per-cell quantities (RP::Cell) compute them once per
+    // cell and take the right cell's from the next lane (as the lean body).
+    constexpr bool PERCELL = HasCell<RP>::value && NCELL + 4 <= 32;
+    const bool fromQx = SPLIT && IXY == 2 && !cflonly;   // split y sweep: the x-swept tile state
+    auto load = [&](double (&q)[MEQN], int kk) {
+        const int ci = cell_i(kk), cj = cell_j(kk);
+        if (fromQx) {
 #pragma unroll
-            for (int m = 0; m < MEQN; m++) {
-                qL[m] = Qx[(m * QROWS + (jL - j0 - QROW0)) * QP + (iL - i0)];
-                qR[m] = Qx[(m * QROWS + (jR - j0 - QROW0)) * QP + (iR - i0)];
-            }
+            for (int m = 0; m < MEQN; m++) q[m] = Qx[(m * QROWS + (cj - j0 - QROW0)) * QP + (ci - i0)];
         } else {
+            const long long o = qoff(a, 0, ci, cj);
 #pragma unroll
-            for (int m = 0; m < MEQN; m++) {
-                qL[m] = qin[oL + m * a.plane];
-                qR[m] = qin[oR + m * a.plane];
-            }
+            for (int m = 0; m < MEQN; m++) q[m] = qin[o + m * a.plane];
         }
-#pragma unroll
-        for (int m = 0; m < MAUX; m++) {
-            auxL[m] = a.aux[oL + m * a.plane];
-            auxR[m] = a.aux[oR + m * a.plane];
-        }
-        RP::template rpn2<IXY>(qL, qR, auxL, auxR, a.prm, wave, s, amdq, apdq, roe);
+    };
+    auto publish = [&](const double (&wave)[MW][MEQN], const double (&s)[MW], const double (&amdq)[MEQN],
+                       const double (&apdq)[MEQN], const double (&roe)[NROE]) {
 #pragma unroll
         for (int p = 0; p < MW; p++) {
 #pragma unroll
@@ -289,9 +287,40 @@ CLAW2_HD void sweep_chunk(const StepArgs& a, Ctx& ctx, const double* qin, double
 #pragma unroll
         for (int r = 0; r < NROE; r++) X(2 * MEQN + r, tid) = roe[r];
         if (a.capa >= 0) {
+            const long long oL = qoff(a, 0, cell_i(k - 1), cell_j(k - 1));
+            const long long oR = oL + (IXY == 1 ? 1 : a.ld);
             dtl = dtn / a.aux[oL + a.capa * a.plane];
             dtr = dtn / a.aux[oR + a.capa * a.plane];
         }
+    };
+    if constexpr (PERCELL) {
+        double qL[MEQN];
+        typename RP::Cell L{};
+        if (lineok && k - 1 <= len + 1) {
+            load(qL, k - 1);
+            L = RP::template cell<IXY>(qL, a.prm);
+        }
+        const typename RP::Cell R = L.map([&](double v) { return ctx.shfl_down(v); });
+        if (ifok) {
+            double qR[MEQN], wave[MW][MEQN], s[MW], amdq[MEQN], apdq[MEQN], roe[NROE];
+            load(qR, k);
+            RP::template rpn2c<IXY>(qL, qR, L, R, a.prm, wave, s, amdq, apdq, roe);
+            publish(wave, s, amdq, apdq, roe);
+        }
+    } else if (ifok) {
+        double qL[MEQN], qR[MEQN], auxL[AUXN], auxR[AUXN];
+        double wave[MW][MEQN], s[MW], amdq[MEQN], apdq[MEQN], roe[NROE];
+        load(qL, k - 1);
+        load(qR, k);
+        const long long oL = qoff(a, 0, cell_i(k - 1), cell_j(k - 1));
+        const long long oR = oL + (IXY == 1 ? 1 : a.ld);      // cell k: one step along the slice
+#pragma unroll
+        for (int m = 0; m < MAUX; m++) {
+            auxL[m] = a.aux[oL + m * a.plane];
+            auxR[m] = a.aux[oR + m * a.plane];
+        }
+        RP::template rpn2<IXY>(qL, qR, auxL, auxR, a.prm, wave, s, amdq, apdq, roe);
+        publish(wave, s, amdq, apdq, roe);
     }
     ctx.syncwarp();
 
