@@ -173,9 +173,10 @@ CLAW2_EXPORT int claw2_step(const claw2_problem* p, const double* q_in, double* 
                const double* aux, double dt, void* scratch, double* cfl_dev,
                void* stream);
 
-/* Largest number of tiles (29x29 cells each, 28x28 with dimensional
- * splitting) that claw2_step_noalloc accepts: ceil(mx/29)*ceil(my/29) <= 32768,
- * i.e. about 27 million cells. */
+/* Largest number of tiles that claw2_step_noalloc accepts (claw2_scratch_bytes
+ * counts them: 29x29 cells for the acoustics solvers, 13x13 on their grids of
+ * fewer than 148 such tiles, 28x28 for Euler and shallow water and with
+ * dimensional splitting): about 25 to 27 million cells. */
 #define CLAW2_NOALLOC_MAX_TILES 32768
 
 /* claw2_step without any device allocation, for callers that may not allocate
