@@ -241,6 +241,24 @@ def test_walled_euler_conserves_mass_and_energy():
         assert abs(s1 - s0) <= 64 * np.finfo(float).eps * np.sum(np.abs(q[m])) * 10, (m, s1 - s0)
 
 
+def test_walled_shallow_water_conserves_mass():
+    """The dam break of config 3 at 192^2 with walls on every side, unsplit
+    and split, through the public API: total depth is conserved to round-off."""
+    import bench
+    from pyclaw_b200 import _abi
+    p, q, run = bench.shallow_config(192)
+    for side in range(2):
+        p.bc_lower[side] = _abi.BC_WALL
+        p.bc_upper[side] = _abi.BC_WALL
+    for split in (False, True):
+        claw, solver = _api_run(p, q, None, run, 0.4, 1, split=split, trans=-1 if split else 2,
+                                rp=pc.riemann.rp2_shallow_roe_with_efix, bounds=((-2.5, 2.5), (-2.5, 2.5)))
+        got = claw.solution.state.q
+        s0, s1 = np.sum(q[0]), np.sum(got[0])
+        assert abs(s1 - s0) <= 64 * np.finfo(float).eps * s0 * 10, (split, s1 - s0)
+        assert solver.status['numsteps'] > 10
+
+
 def test_fixed_dt_too_large_gives_up():
     p, q, aux, run = K.acoustics_homogeneous_setup(mx=40, my=40, split=False)
     x = pc.Dimension('x', -1.0, 1.0, 40)
