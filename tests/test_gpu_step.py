@@ -83,6 +83,40 @@ def test_unsplit_limiters_bit_identical_to_oracle(orc, name, lim, order, tr):
     assert np.array_equal(out, ref)
 
 
+CAPA_FWAVE_CASES = [("vc_acoustics", capa, fw, tr) for capa in (-1, 0, 1) for fw in (0, 1) for tr in (2, 1, 0, -1)
+                    if capa >= 0 or fw]
+CAPA_FWAVE_CASES += [("acoustics", -1, 1, tr) for tr in (2, -1)] + [("euler4", -1, 1, 2), ("shallow", -1, 1, -1)]
+
+
+@pytest.mark.parametrize("name,capa,fwave,tr", CAPA_FWAVE_CASES)
+def test_capacity_and_fwave_branches_bit_identical_to_oracle(orc, name, capa, fwave, tr):
+    """The capacity-function branch (dtdx/kappa per cell, the update divided by
+    kappa; step2.f90:101-105,151-163, flux2.f90) and the f-wave branch of the
+    second-order correction (sign(s) for |s|, flux2.f90:150-162) through the
+    generic tile body, against the oracle.  The solvers here are not f-wave
+    solvers and aux component `capa` is not a physical capacity; the cases
+    exercise the branches' arithmetic, which must agree exactly."""
+    mx, my = 61, 47
+    p = H.problem(name, mx, my, tr, bcl=(1, 3), bcu=(3, 1))
+    p.index_capa = capa
+    p.use_fwave = fwave
+    q, aux = H.init_fields(p, seed=capa * 5 + fwave * 3 + tr + 17)
+    qbc = orc.new_qbc(p, q)
+    orc.fill_ghosts(p, qbc)
+    auxbc = None
+    if p.num_aux:
+        auxbc = orc.new_qbc(p, aux, p.num_aux)
+        orc.fill_aux_ghosts(p, auxbc)
+    dt = 0.25 / max(mx, my)
+    ref = qbc.copy(order="F")
+    cfl_ref = orc.step_hyperbolic(p, ref, auxbc, dt)
+    out, cfl = H.dev_step(p, qbc, auxbc, dt)
+    assert np.array_equal(out[I], ref[I]), np.nanmax(np.abs(out[I] - ref[I]))
+    assert cfl == cfl_ref
+    orc.fill_ghosts(p, ref)
+    assert np.array_equal(out, ref)
+
+
 def test_nonfinite_state_is_reported(orc):
     p = H.problem("euler4", 40, 40, 2)
     q, _ = H.init_fields(p)
