@@ -726,8 +726,12 @@ CLAW2_HD void step_tile_at(const StepArgs& a, Ctx& ctx, const TileId& tile)
             const int clast = (c0 + LPC - 1 < last) ? c0 + LPC - 1 : last;
             sweep_chunk<RP, 1, SPLIT, TX, TY, NT>(a, ctx, qin, Qx, WB, B2, i0, j0, line, c0, clast,
                                                   line <= last, false, dtdx, dtdy, cflm);
-            if (SPLIT) ctx.sync();
+            // split: a line reads and writes only its own row of Qx and its own
+            // warp's slots of WB/B2, so chunks need no block barrier, only a
+            // warp barrier before the next chunk reuses the slots
+            if (SPLIT) ctx.syncwarp();
         }
+        if (SPLIT) ctx.sync();          // the y sweep reads the whole x-swept tile
     }
     // ---- y sweeps: unsplit columns i0-1..i0+TX (cols -1..mx); split the tile's
     //      columns, plus ghost columns -2,-1 / mx,mx+1 (CFL only, step2ds.f90:177)
@@ -757,8 +761,9 @@ CLAW2_HD void step_tile_at(const StepArgs& a, Ctx& ctx, const TileId& tile)
                 }
                 sweep_chunk<RP, 2, SPLIT, TX, TY, NT>(a, ctx, qin, Qx, WB, B2, i0, j0, line, 0, 0,
                                                       l < nlines, cflonly, dtdy, dtdx, cflm);
-                ctx.sync();
+                ctx.syncwarp();         // a y line touches only its own column of Qx
             }
+            ctx.sync();
         }
     }
 
