@@ -207,6 +207,17 @@ def make_solver(pc, prob, run):
 # ---------------------------------------------------------------------------
 # helpers
 # ---------------------------------------------------------------------------
+def _ncu_record(key):
+    """Per-launch counters of one kernel from one ncu capture, kept in
+    profiles/ncu_metrics.json (written from the capture that the profile
+    summary of the same name describes); None if absent."""
+    path = os.path.join(ROOT, "profiles", "ncu_metrics.json")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        return json.load(f).get(key)
+
+
 def _peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(path):
@@ -316,11 +327,19 @@ def _sum_over_ranks(x, world):
 # ---------------------------------------------------------------------------
 # CPU arms (oracle = C restatement of the reference Fortran step)
 # ---------------------------------------------------------------------------
-def cpu_rate(prob, q, run, omp, max_seconds=15.0, max_steps=None):
-    """Time whole-grid oracle steps (BC fill + step + dt control) on the host;
-    returns (cell-updates/s, steps timed, threads, seconds)."""
+def cpu_build():
+    """The host-native timing build of the oracle: (library, its flags, CPU model)."""
     from oracle import oracle as O
-    lib = O.load(omp)
+    lib = O.load(timing=True)
+    return lib, lib.build_flags, lib.cpu_model
+
+
+def cpu_rate(prob, q, run, omp, max_seconds=15.0, max_steps=None):
+    """Time whole-grid oracle steps (BC fill + step + dt control) on the host
+    with the oracle's host-native timing build (-O3 -march=native, FMA
+    allowed); returns (cell-updates/s, steps timed, threads, seconds)."""
+    from oracle import oracle as O
+    lib, _, _ = cpu_build()
     qbc = O.new_qbc(prob, q)
     ctrl = O.control_init(0.0, run['dt_initial'], 1e9, run['cfl_max'], run['cfl_desired'], lib=O.load())
     threads = lib.orc_num_threads() if omp else 1
@@ -332,7 +351,7 @@ def cpu_rate(prob, q, run, omp, max_seconds=15.0, max_steps=None):
         ctrl.done = 0
         ctrl.error = 0
         ctrl.max_steps = ctrl.iter + 1
-        rc = O.evolve(prob, qbc, None, ctrl, omp=omp)
+        rc = O.evolve(prob, qbc, None, ctrl, omp=omp, lib=lib)
         if rc not in (0, 5):
             raise RuntimeError("oracle evolve failed: %d" % rc)
         steps += 1
@@ -349,7 +368,7 @@ def run_reference_arm(args, world, rank):
         return
     prob, q, aux, run, tfinal = shockbubble_config(split=args.split)
     from oracle import oracle as O
-    lib = O.load(True)
+    lib, flags, model = cpu_build()
     qbc = O.new_qbc(prob, q)
     ctrl = O.control_init(0.0, run['dt_initial'], 1e9, run['cfl_max'], run['cfl_desired'], lib=O.load())
     threads = lib.orc_num_threads()
@@ -359,7 +378,7 @@ def run_reference_arm(args, world, rank):
         ctrl.done = 0
         ctrl.error = 0
         ctrl.max_steps = ctrl.iter + 1
-        rc = O.evolve(prob, qbc, None, ctrl, omp=True)
+        rc = O.evolve(prob, qbc, None, ctrl, omp=True, lib=lib)
         if rc not in (0, 5):
             raise RuntimeError("oracle evolve failed: %d" % rc)
 
@@ -382,7 +401,8 @@ def run_reference_arm(args, world, rank):
                        "mode": "dimensional splitting" if args.split else "unsplit"},
         "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": threads, "kind": "port",
                          "sample": "%d whole-grid steps (BC fill + step + dt control) of the 1280x320 "
-                                   "shock bubble, oracle OpenMP gather form, %d threads" % (args.steps, threads)},
+                                   "shock bubble, oracle OpenMP gather form, %d threads" % (args.steps, threads),
+                         "build": flags, "cpu_model": model, "nproc": os.cpu_count()},
         "e2e": {"value": value, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -435,6 +455,15 @@ def run_ours(args, world, rank, local):
     dev.ctrl.copy_(dev.ctrl_host)
     flush = torch.empty(256 * 1024 * 1024 // 8, dtype=torch.float64, device="cuda")   # 256 MB > L2
     _barrier(world)
+    # set-up: run the flow on to a developed state (the shock through the
+    # bubble), so that the timed steps see the run's mix of shocked, smooth and
+    # still cells rather than the first steps from t = 0
+    if args.develop > 0:
+        advance(args.develop)
+        torch.cuda.synchronize()
+    dev.ctrl_host.copy_(dev.ctrl)
+    torch.cuda.synchronize()
+    t_timed0 = host.t
 
     for _ in range(max(3, args.warmup)):
         flush.fill_(1.0)
@@ -475,30 +504,43 @@ def run_ours(args, world, rank, local):
     alg_bytes = 8 * (2 * prob.num_eqn + prob.num_aux) * cells   # per launch (one step)
     avg_kernel_s = t_dev / args.steps
     achieved = alg_bytes / avg_kernel_s / 1e9
-    traffic = None
-    tpath = os.path.join(ROOT, "profiles", "step_kernel_split_euler1280x320.md" if args.split
-                         else "lean_step_kernel_euler1280x320.md")
-    if os.path.exists(tpath):            # dram read+write bytes of one launch, from the ncu capture
-        with open(tpath) as f:
-            for ln in f:
-                if ln.startswith("traffic_bytes_per_launch:"):
-                    traffic = int(ln.split(":")[1])
+    rec = _ncu_record("step_kernel_split_euler1280x320" if args.split else "lean_step_kernel_euler1280x320")
+    traffic = (rec["dram_bytes_read"] + rec["dram_bytes_write"]) if rec else None
+    # FP64 pipe: the step's real bound (about 1,900 FP64 instructions per cell,
+    # IEEE divisions and square roots, no FMA contraction): lane-slots of the
+    # FP64 pipe used per launch (ncu warp instructions x 32) per second, against
+    # SMs x 64 FP64 lanes x the SM clock
+    fp64 = None
+    if rec and rec.get("fp64_pipe_warp_inst"):
+        nsm = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+        f_mhz = (clk or {}).get("sm_max_mhz") or 1965.0
+        lanes = 32.0 * rec["fp64_pipe_warp_inst"]
+        fp64 = {"achieved": lanes / avg_kernel_s / 1e12, "peak": nsm * 64 * f_mhz * 1e6 / 1e12,
+                "unit": "T FP64 lane-ops/s", "frac": None,
+                "fp64_lane_ops_per_launch": lanes, "fp64_lane_ops_per_cell": lanes / cells,
+                "source": "ncu smsp__inst_executed_pipe_fp64.sum x 32 of one launch (%s); peak = %d SMs x 64 "
+                          "FP64 lanes x %.0f MHz" % (rec.get("capture", "profiles/ncu_metrics.json"), nsm, f_mhz)}
+        fp64["frac"] = fp64["achieved"] / fp64["peak"]
 
     # ---- e2e through the host-buffer C ABI (claw2_session_evolve) ----------
-    e2e = None
+    e2e = e2e_s2 = None
     if rank == 0 or world > 1:
         e2e = _e2e(lib, prob, q, run, args)
+        e2e_s2 = _e2e_step2(lib, prob, q, run, args)
     e2e_val = _sum_over_ranks(e2e["value"], world) if e2e else None
+    e2e_s2_val = _sum_over_ranks(e2e_s2["value"], world) if e2e_s2 else None
 
     # ---- CPU baseline (oracle, all host threads; bounded sample) ---------------
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         rate, n, thr, el = cpu_rate(prob, q, run, omp=True, max_seconds=12.0)
         rate1, n1, _, el1 = cpu_rate(prob, q, run, omp=False, max_seconds=8.0)
+        _, flags, model = cpu_build()
         cpu = {"value": rate, "unit": "cell-updates/s", "cores": thr, "kind": "port",
-               "sample": "%d whole-grid steps (%.1f s) of the 1280x320 shock bubble through the oracle's "
-                         "OpenMP gather form on %d threads; serial oracle: %.4g cell-updates/s over %d steps"
-                         % (n, el, thr, rate1, n1)}
+               "sample": "%d whole-grid steps (%.1f s) of the 1280x320 shock bubble from t = 0 through the "
+                         "oracle's OpenMP gather form on %d threads; serial: %.4g cell-updates/s over %d steps"
+                         % (n, el, thr, rate1, n1),
+               "serial_value": rate1, "build": flags, "cpu_model": model, "nproc": os.cpu_count()}
 
     if rank == 0:
         line = {
@@ -513,22 +555,44 @@ def run_ours(args, world, rank, local):
                                        "NCCL halo exchange + CFL max all-reduce per step" % (world, 320 * world))
                        if world > 1 else "single",
                        "l2": "flushed (256 MB write) before every timed step",
+                       "develop_steps": int(args.develop), "t_first_timed_step": t_timed0,
                        "accepted_steps": int(accepted)},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
+                         "traffic_note": "dram read+write of one cold ncu launch; most of the 13 MB of results "
+                                         "stay resident in L2 during the launch" if traffic else None,
                          "peak_source": peak_kind,
-                         "algorithmic_bytes_per_launch": alg_bytes},
+                         "algorithmic_bytes_per_launch": alg_bytes,
+                         "fp64": fp64},
             "cpu_baseline": cpu,
             # one call = one output interval of Controller.run: the state goes up
             # once, the steps of the interval run on the device, the state comes back
             "e2e": {"value": e2e_val, "unit": "cell-updates/s",
                     "h2d_bytes_per_step": e2e["h2d"] / e2e["steps"], "d2h_bytes_per_step": e2e["d2h"] / e2e["steps"],
                     "h2d_bytes_per_call": e2e["h2d"], "d2h_bytes_per_call": e2e["d2h"],
-                    "steps_per_call": e2e["steps"], "calls": e2e["calls"]} if e2e else None,
+                    "steps_per_call": e2e["steps"], "calls": e2e["calls"],
+                    "api": "claw2_session_evolve (one Controller.run output interval per call; the steps of a "
+                           "call run back to back, L2 not flushed)",
+                    "per_step_f2py_contract": {
+                        "value": e2e_s2_val, "unit": "cell-updates/s", "api": "claw2_session_step2",
+                        "h2d_bytes_per_step": e2e_s2["h2d"], "d2h_bytes_per_step": e2e_s2["d2h"],
+                        "steps": e2e_s2["steps"]} if e2e_s2 else None} if e2e else None,
             "gpu_launches": int(args.steps),
             "clocks": clk,
             "wall_s": wall,
         }
+        if world == 1 and not args.headline_only:
+            # the metric's other parts, each measured in its own timed region
+            # with its own clock record: the batched form and the adjoint
+            # against the plain step, and configs 1 and 3
+            line["workloads"] = {}
+            for name, fn in (("batched", run_batched), ("adjoint", run_adjoint), ("shallow", run_shallow),
+                             ("acoustics", run_acoustics)):
+                try:
+                    line["workloads"][name] = fn(args)
+                except Exception as e:          # one failing part must not cost the headline line
+                    line["workloads"][name] = {"error": "%s: %s" % (type(e).__name__, e)}
+                torch.cuda.empty_cache()
         print(json.dumps(line), flush=True)
 
 
@@ -566,6 +630,65 @@ def _e2e(lib, prob, q, run, args):
         lib.claw2_session_destroy(s)
 
 
+def _ghosted(prob, q):
+    """q with two ghost layers filled as Solver.apply_q_bcs does
+    (src/pyclaw/solver.py:368-434): x sides over all rows, then y sides over
+    all columns; extrapolation copies the edge cell, a wall mirrors and negates
+    the normal momentum.  Only the extrapolation and wall sides of the
+    shock-bubble workload are needed here."""
+    g = 2
+    qbc = np.zeros((q.shape[0], q.shape[1] + 2 * g, q.shape[2] + 2 * g), order='F')
+    qbc[:, g:-g, g:-g] = q
+    for axis in (0, 1):
+        for side, bc in ((0, int(prob.bc_lower[axis])), (1, int(prob.bc_upper[axis]))):
+            n = q.shape[1 + axis]
+            for k in range(g):
+                dst = g - 1 - k if side == 0 else n + g + k
+                if bc == 1:                                   # extrapolation
+                    src = g if side == 0 else n + g - 1
+                elif bc == 3:                                 # wall
+                    src = g + k if side == 0 else n + g - 1 - k
+                else:
+                    raise ValueError("only extrapolation and wall sides here")
+                a = qbc[:, dst, :] if axis == 0 else qbc[:, :, dst]
+                a[...] = qbc[:, src, :] if axis == 0 else qbc[:, :, src]
+                if bc == 3:
+                    a[1 + axis] = -a[1 + axis]
+    return qbc
+
+
+def _e2e_step2(lib, prob, q, run, args):
+    """claw2_session_step2, the per-step f2py contract of step2: every call
+    copies the ghosted state in the reference's layout from pinned host
+    memory, converts it, takes one step, converts back and copies the result
+    and the CFL number to the host."""
+    import torch
+    from pyclaw_b200 import _lib
+    s = ctypes.c_void_p()
+    _lib.check(lib.claw2_session_create(ctypes.byref(prob), ctypes.byref(s)), "claw2_session_create")
+    try:
+        qbc = _ghosted(prob, q)
+        bufs = [torch.from_numpy(qbc.ravel(order='F')).clone().pin_memory() for _ in range(2)]
+        arrs = [b.numpy() for b in bufs]
+        cfl = ctypes.c_double()
+        dt = run['dt_initial']
+
+        def call(k):
+            return lib.claw2_session_step2(s, arrs[k & 1].ctypes.data, arrs[(k + 1) & 1].ctypes.data, None, dt,
+                                           ctypes.byref(cfl))
+        for k in range(2):
+            _lib.check(call(k), "claw2_session_step2")      # warm-up
+        n = max(4, min(args.steps, 40))
+        t0 = time.perf_counter()
+        for k in range(n):
+            _lib.check(call(k), "claw2_session_step2")
+        el = time.perf_counter() - t0
+        nbytes = 8 * prob.num_eqn * (prob.mx + 4) * (prob.my + 4)
+        return {"value": n * prob.mx * prob.my / el, "h2d": nbytes, "d2h": nbytes + 8, "steps": n}
+    finally:
+        lib.claw2_session_destroy(s)
+
+
 def run_batched(args):
     """Config 4: 1024 uneven vc-acoustics instances, 300 controlled steps each:
     the batched persistent kernel (autotuned, CUDA graph) against looping the
@@ -582,11 +705,15 @@ def run_batched(args):
     bs.init_controls([i["dt"] for i in insts], max_steps=nsteps)
     bs.advance_graph(0)
     torch.cuda.synchronize()
+    clocks = ClockSampler(torch.cuda.current_device())
+    clocks.start()
+    time.sleep(0.3)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
     bs.advance_graph(nsteps, chunk=50)
     e1.record()
     torch.cuda.synchronize()
+    clk = clocks.stop()
     t_batch = e0.elapsed_time(e1) / 1e3
     ctrls = bs.controls()
     if not all(c.done for c in ctrls):
@@ -595,9 +722,13 @@ def run_batched(args):
     # looped plain step: each instance alone through the device-controlled loop
     lib = _lib.load()
     t_loop = 0.0
+    t_loop_dev = 0.0
     upd_loop = 0
     check = {0, len(insts) // 2, len(insts) - 1}
     same = True
+    clocks = ClockSampler(torch.cuda.current_device())
+    clocks.start()
+    time.sleep(0.3)
     for k, inst in enumerate(insts):
         pk = bs.problems[k]
         dev = DeviceState(pk)
@@ -606,13 +737,19 @@ def run_batched(args):
         c = _abi.Control()
         lib.claw2_control_init(ctypes.byref(c), 0.0, inst["dt"], 1e300, 1.0, 0.9, 1e99, 1, 0, nsteps, 0.9)
         torch.cuda.synchronize()
+        d0, d1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         w0 = time.perf_counter()
+        d0.record()
         out = dev.evolve(c)
+        d1.record()
         t_loop += time.perf_counter() - w0
+        torch.cuda.synchronize()
+        t_loop_dev += d0.elapsed_time(d1) / 1e3
         upd_loop += out.numsteps * cells[k]
         if k in check:
             same = same and bool(np.array_equal(dev.download_q(), bs.solution(k)))
         del dev
+    clk_loop = clocks.stop()
     line = {
         "metric": "cell_updates_per_s", "value": upd_batch / t_batch, "unit": "cell-updates/s", "n_gpus": 1,
         "steps": nsteps, "higher_is_better": True, "dtype": "f64", "data": "synthetic",
@@ -620,10 +757,15 @@ def run_batched(args):
                    "cells_total": int(sum(cells)), "tiles": bs.ntiles, "autotune": tuning},
         "batched_seconds": t_batch, "looped_seconds": t_loop,
         "looped_value": upd_loop / t_loop, "speedup_vs_looped_plain_step": (upd_batch / t_batch) / (upd_loop / t_loop),
+        "timing": "batched: CUDA events around the graph replays; looped: host wall time of each instance's "
+                  "device-controlled loop (launches, controller polls), its device time beside it",
+        "looped_device_seconds": t_loop_dev,
+        "speedup_vs_looped_device_time": (upd_batch / t_batch) / (upd_loop / t_loop_dev),
         "spot_check_bit_identical": same,
+        "clocks": clk, "clocks_looped": clk_loop,
     }
-    print(json.dumps(line), flush=True)
     bs.close()
+    return line
 
 
 def run_batched_sharded(args, world, rank):
@@ -743,7 +885,7 @@ def run_shallow(args):
                      "traffic": None, "peak_kind": peak_kind},
         "clocks": clk, "cpu_baseline": cpu,
     }
-    print(json.dumps(line), flush=True)
+    return line
 
 
 def run_acoustics(args):
@@ -777,7 +919,11 @@ def run_acoustics(args):
 
     for _ in range(max(1, args.warmup // 3)):
         once()
+    clocks = ClockSampler(torch.cuda.current_device())
+    clocks.start()
+    time.sleep(0.3)
     out, t = once()
+    clk = clocks.stop()
     if out.error:
         raise RuntimeError("device loop error %d" % out.error)
     value = out.numsteps * cells / t
@@ -794,9 +940,9 @@ def run_acoustics(args):
         "config": {"workload": "acoustics_256x256_walls_t0.6", "solver": "acoustics", "limiter": "MC",
                    "transverse_waves": 2, "t_final": out.t, "run_seconds": t,
                    "timing": "whole run to t=0.6 incl. the host polling of the controller every batch of steps"},
-        "cpu_baseline": cpu,
+        "cpu_baseline": cpu, "clocks": clk,
     }
-    print(json.dumps(line), flush=True)
+    return line
 
 
 def run_adjoint(args):
@@ -855,8 +1001,12 @@ def run_adjoint(args):
         once()
         for x in (rho, K, p0):
             x.grad = None
+    clocks = ClockSampler(torch.cuda.current_device())
+    clocks.start()
+    time.sleep(0.3)
     t_plain = min(plain_forward() for _ in range(2))
     loss, t_fwd, t_bwd = once()
+    clk = clocks.stop()
     g_rho, g_K, g_p0 = (x.grad for x in (rho, K, p0))
     cells = n * n * S * cfg["nsteps"]
     line = {
@@ -871,8 +1021,9 @@ def run_adjoint(args):
         "loss": loss,
         "grad_norms": {"rho": float(g_rho.norm()), "K": float(g_K.norm()), "p0": float(g_p0.norm())},
         "grad_finite": bool(torch.isfinite(g_rho).all() and torch.isfinite(g_K).all() and torch.isfinite(g_p0).all()),
+        "clocks": clk,
     }
-    print(json.dumps(line), flush=True)
+    return line
 
 
 def main():
@@ -882,6 +1033,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--headline-only", action="store_true",
+                    help="only the shock-bubble line, without the batched / adjoint / shallow / acoustics parts")
+    ap.add_argument("--develop", type=int, default=1000,
+                    help="untimed steps of set-up before the warm-up (shock bubble)")
     ap.add_argument("--split", action="store_true",
                     help="shock bubble with dimensional splitting (the reference's default mode)")
     ap.add_argument("--workload", default="shockbubble", choices=["shockbubble", "batched", "adjoint", "shallow", "acoustics"])
@@ -898,16 +1053,16 @@ def main():
             if world > 1:
                 run_batched_sharded(args, world, rank)
             elif rank == 0:
-                run_batched(args)
+                print(json.dumps(run_batched(args)), flush=True)
         elif args.workload == "adjoint":
             if rank == 0:
-                run_adjoint(args)
+                print(json.dumps(run_adjoint(args)), flush=True)
         elif args.workload == "shallow":
             if rank == 0:
-                run_shallow(args)
+                print(json.dumps(run_shallow(args)), flush=True)
         elif args.workload == "acoustics":
             if rank == 0:
-                run_acoustics(args)
+                print(json.dumps(run_acoustics(args)), flush=True)
         elif args.impl == "reference":
             run_reference_arm(args, world, rank)
         else:

@@ -179,6 +179,14 @@ CLAW2_EXPORT int claw2_step(const claw2_problem* p, const double* q_in, double* 
  * dimensional splitting): about 25 to 27 million cells. */
 #define CLAW2_NOALLOC_MAX_TILES 32768
 
+/* For testing the bounded wait of the TMA-staged tile bodies only (no
+ * counterpart in the reference): from now on every such CTA of this process
+ * waits for `bytes` (a multiple of 8, at most 65536; 0 restores normal
+ * operation) more than its halo copies deliver, so its wait on the copies runs
+ * out after about a second; the step then reports CLAW2_ERR_TIMEOUT through
+ * the controller (a NaN CFL number without one) and writes no cells. */
+CLAW2_EXPORT int claw2_debug_halo_shortfall(int bytes);
+
 /* claw2_step without any device allocation, for callers that may not allocate
  * GPU memory (their memory belongs to a pool they manage, their time loop must
  * not call the allocator, or their language binding cannot own device memory).
@@ -190,7 +198,10 @@ CLAW2_EXPORT int claw2_step(const claw2_problem* p, const double* q_in, double* 
  * stream capture begins.  Problems with more tiles than the maximum return
  * CLAW2_ERR_SIZE.  All calls share the one array, so calls that overlap on the
  * GPU (different streams, or different host threads, on the same device) race;
- * order them on one stream. */
+ * order them on one stream.  The address is remembered per device ordinal for
+ * the device's primary context (the one the CUDA runtime uses): do not call
+ * this entry point with another driver-API context current, nor after a
+ * cudaDeviceReset of a device it has already run on. */
 CLAW2_EXPORT int claw2_step_noalloc(const claw2_problem* p, const double* q_in, double* q_out,
                                     const double* aux, double dt, double* cfl_dev, void* stream);
 

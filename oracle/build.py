@@ -11,9 +11,22 @@ Compiles claw2_oracle.c into two shared libraries next to this file:
                           parity build; the tests check that).  No -march flag,
                           so the library runs on any x86-64 host it travels to.
 
+A third library is only ever built on the machine that times the CPU
+baseline, by ``build_timing()``:
+
+  liboracle_claw2_native_<key>.so  -O3 -march=native -fopenmp with the compiler's
+                          default floating-point contraction (FMA allowed):
+                          the fastest build of the same source for this host,
+                          used for timing only, never for parity.  <key> is a
+                          hash of the host's CPU model and feature flags and of
+                          the compiler, so a copy built on another machine is
+                          never loaded here.
+
 Run as ``python oracle/build.py`` or call ``build()``.
 """
+import hashlib
 import os
+import platform
 import subprocess
 import sys
 
@@ -49,6 +62,45 @@ def build(force=False, verbose=False):
             subprocess.run(cmd, check=True)
             os.replace(tmp, out)
     return LIB, LIB_OMP
+
+
+TIMING_FLAGS = ["-O3", "-march=native", "-fopenmp", "-DORC_OPENMP", "-fPIC", "-shared", "-fno-fast-math",
+                "-std=gnu11", "-w"]
+
+
+def host_cpu():
+    """(model name, feature-flags line) of this host's first CPU."""
+    model, flags = platform.processor() or "unknown", ""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for ln in f:
+                if ln.startswith("model name") and model in ("unknown", "x86_64", ""):
+                    model = ln.split(":", 1)[1].strip()
+                elif ln.startswith("flags") and not flags:
+                    flags = ln.split(":", 1)[1].strip()
+                if flags and model not in ("unknown", "x86_64", ""):
+                    break
+    except OSError:
+        pass
+    return model, flags
+
+
+def build_timing(verbose=False):
+    """Compile (if needed) the host-native timing build; returns (path, flags, cpu model)."""
+    model, flags = host_cpu()
+    try:
+        cc = subprocess.run(["gcc", "--version"], capture_output=True, text=True).stdout.splitlines()[0]
+    except (OSError, IndexError):
+        cc = "gcc"
+    key = hashlib.sha1(("%s|%s|%s|%s" % (model, flags, cc, " ".join(TIMING_FLAGS))).encode()).hexdigest()[:12]
+    out = os.path.join(HERE, "liboracle_claw2_native_%s.so" % key)
+    if _stale(out):
+        cmd = ["gcc"] + TIMING_FLAGS + ["-o", out + ".tmp", SRC, "-lm"]
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.run(cmd, check=True)
+        os.replace(out + ".tmp", out)
+    return out, "gcc " + " ".join(TIMING_FLAGS) + " (" + cc + ")", model
 
 
 if __name__ == "__main__":

@@ -24,14 +24,23 @@ from pyclaw_b200 import _abi  # noqa: E402  (plain ctypes structs, no CUDA)
 _LIBS = {}
 
 
-def load(omp=False):
-    """Load (building if needed) the parity or the OpenMP oracle library."""
-    key = "omp" if omp else "serial"
+def load(omp=False, timing=False):
+    """Load (building if needed) the parity or the OpenMP oracle library, or
+    with timing=True the host-native timing build (FMA allowed: for timing
+    the CPU baseline only, never for parity; it has both the serial and the
+    OpenMP entry points)."""
+    key = "timing" if timing else ("omp" if omp else "serial")
     if key in _LIBS:
         return _LIBS[key]
     from oracle import build as _build  # noqa: WPS433
-    lib_path, omp_path = _build.build()
-    lib = ctypes.CDLL(omp_path if omp else lib_path)
+    if timing:
+        path, flags, model = _build.build_timing()
+        lib = ctypes.CDLL(path)
+        lib.build_flags, lib.cpu_model = flags, model
+        omp = True
+    else:
+        lib_path, omp_path = _build.build()
+        lib = ctypes.CDLL(omp_path if omp else lib_path)
     P = ctypes.POINTER(_abi.Problem)
     dp = ctypes.POINTER(ctypes.c_double)
     C = ctypes.POINTER(_abi.Control)

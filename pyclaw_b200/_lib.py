@@ -31,6 +31,7 @@ PROTOTYPES = [
     ("claw2_fill_aux_ghosts", ctypes.c_int, [_P, _dp, _vp]),
     ("claw2_step", ctypes.c_int, [_P, _dp, _dp, _dp, _dbl, _vp, _dp, _vp]),
     ("claw2_step_noalloc", ctypes.c_int, [_P, _dp, _dp, _dp, _dbl, _dp, _vp]),
+    ("claw2_debug_halo_shortfall", ctypes.c_int, [ctypes.c_int]),
     ("claw2_advance", ctypes.c_int, [_P, _dp, _dp, _dp, _vp, _vp, ctypes.c_int, _vp]),
     ("claw2_advance_hooked", ctypes.c_int, [_P, _dp, _dp, _dp, _vp, _vp, ctypes.c_int, ctypes.POINTER(_abi.Hooks),
                                             _vp]),

@@ -21,9 +21,11 @@ SRCS = [os.path.join(HERE, "csrc", "claw2_capi.cu"),
         os.path.join(HERE, "csrc", "claw2_adjoint.cu")]
 OBJDIR = os.path.join(HERE, "_build")
 DEPS = SRCS + [os.path.join(HERE, "csrc", "claw2_kernels.cuh"),
+               os.path.join(HERE, "csrc", "claw2_devattr.h"),
                os.path.join(HERE, "csrc", "claw2_riemann.cuh"),
                os.path.join(HERE, "csrc", "claw2_light.cuh"),
                os.path.join(HERE, "csrc", "claw2_lean.cuh"),
+               os.path.join(HERE, "csrc", "claw2_tma.cuh"),
                os.path.join(ROOT, "include", "claw2.h"),
                os.path.join(ROOT, "include", "claw2_adjoint.h")]
 

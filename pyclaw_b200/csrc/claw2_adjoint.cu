@@ -34,6 +34,7 @@
 #define CLAW2_EXPORT __attribute__((visibility("default")))
 #include "../../include/claw2.h"
 #include "../../include/claw2_adjoint.h"
+#include "claw2_devattr.h"
 #include "claw2_kernels.cuh"
 #include "claw2_light.cuh"
 
@@ -699,13 +700,8 @@ int claw2_shots_step(const claw2_problem* p, int nshots, long long shot_stride, 
     a.partials = reinterpret_cast<double*>(static_cast<char*>(scratch) + tickets);
     a.cfl_out = cfl_dev;
     using SM = LightSmem<FT, FT, 256>;
-    static bool configured = false;
-    if (!configured) {
-        if (cudaFuncSetAttribute(shots_step_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SM::bytes) !=
-            cudaSuccess)
-            return CLAW2_ERR_CUDA;
-        configured = true;
-    }
+    static std::atomic<uint64_t> optin{0};
+    if (smem_optin(optin, shots_step_kernel, SM::bytes) != cudaSuccess) return CLAW2_ERR_CUDA;
     int nbx, nby;
     ftiles(p, &nbx, &nby);
     shots_step_kernel<<<dim3(nbx, nby, nshots), 256, SM::bytes, Sx(stream)>>>(a, shot_stride);
@@ -747,12 +743,8 @@ int claw2_shots_adjoint_step(const claw2_problem* p, int nshots, long long shot_
     a.order = p->order; a.trans = p->transverse;
     a.mthlim[0] = p->mthlim[0]; a.mthlim[1] = p->mthlim[1];
     constexpr int smem = (5 * AR * AR + 2 * 4 * ANT + YF * YR * YP) * 8;
-    static bool configured = false;
-    if (!configured) {
-        if (cudaFuncSetAttribute(adjoint_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
-            return CLAW2_ERR_CUDA;
-        configured = true;
-    }
+    static std::atomic<uint64_t> optin{0};
+    if (smem_optin(optin, adjoint_kernel, smem) != cudaSuccess) return CLAW2_ERR_CUDA;
     const dim3 grid((p->mx + AT - 1) / AT, (p->my + AT - 1) / AT, nshots);
     adjoint_kernel<<<grid, ANT, smem, Sx(stream)>>>(a);
     return cudaGetLastError() == cudaSuccess ? CLAW2_OK : CLAW2_ERR_CUDA;

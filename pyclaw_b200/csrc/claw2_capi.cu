@@ -2,6 +2,8 @@
 //
 // Built for sm_100a with --fmad=false (no FMA contraction, so the step
 // reproduces the reference's operation-by-operation rounding).
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <atomic>
@@ -13,6 +15,7 @@
 
 #define CLAW2_EXPORT __attribute__((visibility("default")))
 #include "../../include/claw2.h"
+#include "claw2_devattr.h"
 #include "claw2_kernels.cuh"
 #include "claw2_light.cuh"
 #include "claw2_lean.cuh"
@@ -75,14 +78,18 @@ template <> struct HasLean<RpShallow> { static constexpr bool value = true; };
 // lean tiles: 28 x 28 cells, so that a line's 32 lanes hold its 32 cells
 constexpr int LTX = 28, LTY = 28;
 
+// tm0 / tm1: tensor maps of the input state (see lean_tile_at), passed as
+// __grid_constant__ parameters so the TMA unit can read them in place.
 template <class RP>
-__global__ void __launch_bounds__(256, CLAW2_LEAN_MINB) lean_step_kernel(StepArgs a)
+__global__ void __launch_bounds__(256, CLAW2_LEAN_MINB)
+lean_step_kernel(StepArgs a, const __grid_constant__ CUtensorMap tm0, const __grid_constant__ CUtensorMap tm1)
 {
     extern __shared__ double smem_dyn[];
+    __shared__ __align__(8) uint64_t halo_bar;
     DevCtx ctx{smem_dyn};
     const TileId t{(int)blockIdx.x, (int)blockIdx.y, (int)gridDim.x, (int)gridDim.y,
                    (int)(blockIdx.y * gridDim.x + blockIdx.x), (int)(gridDim.x * gridDim.y)};
-    lean_tile_at<RP, LTX, LTY, 256>(a, ctx, t);
+    lean_tile_at<RP, LTX, LTY, 256>(a, ctx, t, &tm0, &tm1, &halo_bar);
 }
 
 // Instance of tile t: the last one with tile_begin <= t (binary search).
@@ -364,12 +371,8 @@ int launch_light_t(const StepArgs& a, int nbx, int nby, cudaStream_t st)
 {
     using SM = LightSmem<T, T, 256>;
     auto kern = light_step_kernel<RP, T>;
-    static bool configured = false;
-    if (!configured) {
-        if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SM::bytes) != cudaSuccess)
-            return CLAW2_ERR_CUDA;
-        configured = true;
-    }
+    static std::atomic<uint64_t> optin{0};
+    if (smem_optin(optin, kern, SM::bytes) != cudaSuccess) return CLAW2_ERR_CUDA;
     kern<<<dim3(nbx, nby), 256, SM::bytes, st>>>(a);
     return cudaGetLastError() == cudaSuccess ? CLAW2_OK : CLAW2_ERR_CUDA;
 }
@@ -382,18 +385,59 @@ int launch_light(const StepArgs& a, int nbx, int nby, cudaStream_t st)
     return launch_light_t<RP, 29>(a, nbx, nby, st);
 }
 
-template <class RP>
-int launch_lean(const StepArgs& a, int nbx, int nby, cudaStream_t st)
+// cuTensorMapEncodeTiled from the driver, found through the runtime (no link
+// against libcuda, so the library still loads on a machine without a GPU)
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
 {
+    static std::atomic<void*> fn{nullptr};
+    void* f = fn.load(std::memory_order_acquire);
+    if (!f) {
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess || !f)
+            return nullptr;
+        fn.store(f, std::memory_order_release);
+    }
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+}
+
+// Tensor map of one state buffer for the lean body's halo boxes: the ghosted
+// planes (mx+4 columns, my+4 rows, meqn fields; rows ld doubles apart, planes
+// `plane` doubles apart), boxes of 16 x 32 x meqn, 128-byte swizzle, zeros
+// outside the ghosted array.
+int halo_tensor_map(CUtensorMap* m, const double* q, const StepArgs& a, int meqn)
+{
+    auto encode = tensor_map_encoder();
+    if (!encode) return CLAW2_ERR_CUDA;
+    if ((reinterpret_cast<uintptr_t>(q) & 15u) != 0) return CLAW2_ERR_INVALID;
+    const cuuint64_t dims[3] = {(cuuint64_t)(a.mx + 2 * CLAW2_NUM_GHOST), (cuuint64_t)(a.my + 2 * CLAW2_NUM_GHOST),
+                                (cuuint64_t)meqn};
+    const cuuint64_t strides[2] = {(cuuint64_t)a.ld * sizeof(double), (cuuint64_t)a.plane * sizeof(double)};
+    const cuuint32_t box[3] = {16, 32, (cuuint32_t)meqn};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    const CUresult r = encode(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<double*>(q), dims, strides, box, estr,
+                              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? CLAW2_OK : CLAW2_ERR_CUDA;
+}
+
+// bytes of halo that lean-body CTAs wait for in vain (claw2_debug_halo_shortfall)
+std::atomic<int> g_halo_shortfall{0};
+
+template <class RP>
+int launch_lean(const StepArgs& a0, int nbx, int nby, cudaStream_t st)
+{
+    StepArgs a = a0;
+    a.halo_shortfall = g_halo_shortfall.load(std::memory_order_relaxed);
     using SM = LeanSmem<RP, LTX, LTY, 256>;
     auto kern = lean_step_kernel<RP>;
-    static bool configured = false;
-    if (!configured) {
-        if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SM::bytes) != cudaSuccess)
-            return CLAW2_ERR_CUDA;
-        configured = true;
-    }
-    kern<<<dim3(nbx, nby), 256, SM::bytes, st>>>(a);
+    static std::atomic<uint64_t> optin{0};
+    if (smem_optin(optin, kern, SM::bytes) != cudaSuccess) return CLAW2_ERR_CUDA;
+    CUtensorMap tm0, tm1;
+    int rc = halo_tensor_map(&tm0, a.ctrl ? a.q0 : a.qin, a, RP::MEQN);
+    if (!rc) rc = a.ctrl ? halo_tensor_map(&tm1, a.q1, a, RP::MEQN) : (tm1 = tm0, CLAW2_OK);
+    if (rc) return rc;
+    kern<<<dim3(nbx, nby), 256, SM::bytes, st>>>(a, tm0, tm1);
     return cudaGetLastError() == cudaSuccess ? CLAW2_OK : CLAW2_ERR_CUDA;
 }
 
@@ -407,12 +451,8 @@ int launch_step_t(const StepArgs& a, int nbx, int nby, cudaStream_t st)
     constexpr int TX = SPLIT ? STX : UTX, TY = SPLIT ? STY : UTY, NT = SPLIT ? SNT : UNT;
     using SM = TileSmem<RP, TX, TY, NT, SPLIT>;
     auto kern = step_kernel<RP, TX, TY, NT, SPLIT>;
-    static bool configured = false;
-    if (!configured) {
-        if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SM::bytes) != cudaSuccess)
-            return CLAW2_ERR_CUDA;
-        configured = true;
-    }
+    static std::atomic<uint64_t> optin{0};
+    if (smem_optin(optin, kern, SM::bytes) != cudaSuccess) return CLAW2_ERR_CUDA;
     kern<<<dim3(nbx, nby), NT, SM::bytes, st>>>(a);
     return cudaGetLastError() == cudaSuccess ? CLAW2_OK : CLAW2_ERR_CUDA;
 }
@@ -489,6 +529,13 @@ int conv(const claw2_problem* p, int ncomp, const double* src, double* dst, bool
 extern "C" {
 
 int claw2_abi_version(void) { return CLAW2_ABI_VERSION; }
+
+int claw2_debug_halo_shortfall(int bytes)
+{
+    if (bytes < 0 || bytes > 65536 || (bytes & 7)) return CLAW2_ERR_INVALID;
+    g_halo_shortfall.store(bytes, std::memory_order_relaxed);
+    return CLAW2_OK;
+}
 
 const char* claw2_strerror(int status)
 {
@@ -747,17 +794,10 @@ int batch_launch_t(const StepArgs& common, const claw2_batch_instance* inst, int
 {
     constexpr int SMB = LIGHT ? LightSmem<29, 29, NT>::bytes : TileSmem<RP, 29, 29, NT, false>::bytes;
     auto kern = batch_kernel<RP, NT, MINB, LIGHT>;
-    static int grid = 0;
-    if (grid == 0) {
-        if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SMB) != cudaSuccess)
-            return CLAW2_ERR_CUDA;
-        int dev = 0, nsm = 0, occ = 0;
-        if (cudaGetDevice(&dev) != cudaSuccess ||
-            cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, NT, SMB) != cudaSuccess || occ < 1)
-            return CLAW2_ERR_CUDA;
-        grid = nsm * occ;
-    }
+    static std::atomic<uint64_t> optin{0};
+    static std::atomic<int> grids[kDevAttrSlots];
+    const int grid = persistent_grid(optin, grids, kern, NT, SMB);
+    if (grid < 1) return CLAW2_ERR_CUDA;
     const int g = ntiles < grid ? ntiles : grid;
     for (int n = 0; n < nsteps; n++) {
         kern<<<g, NT, SMB, st>>>(inst, ninst, ntiles, common);

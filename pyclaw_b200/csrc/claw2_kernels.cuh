@@ -57,6 +57,8 @@ struct StepArgs {
     int src, src_aux;      // source term fused into the final write (claw2_source)
     int ctrl_readonly;     // controlled mode that reports the CFL (cfl_out, +inf if
                            // non-finite) instead of updating ctrl (domain decomposition)
+    int halo_shortfall;    // bytes more than its halo copies deliver that a lean-body CTA
+                           // waits for (0; set only to test the bounded wait)
 };
 
 template <int IXY> struct Phase;
@@ -104,8 +106,8 @@ CLAW2_HD double philim(double a, double b, int meth)
 CLAW2_HD void control_update(claw2_control* c, double cfl, int nonfinite)
 {
     c->cfl = cfl;
-    if (nonfinite) {
-        c->error = CLAW2_ERR_NONFINITE;
+    if (nonfinite) {                     // 1: non-finite state, 2: a tile's input never arrived
+        c->error = nonfinite == 2 ? CLAW2_ERR_TIMEOUT : CLAW2_ERR_NONFINITE;
         c->done = 1;
         c->iter++;
         return;
@@ -609,14 +611,17 @@ CLAW2_HD void euler_radial_source(double (&v)[MEQN], double rad, double gamma1, 
     }
 }
 
-// QP: row pitch of Qx in doubles (TX unless the body pads its rows)
+// QP: row pitch of Qx in doubles (TX unless the body pads its rows).
+// fault: the tile could not be computed (its input never arrived): nothing is
+// written and the step reports CLAW2_ERR_TIMEOUT (controlled mode) or a NaN
+// CFL number.
 template <int MEQN, int TX, int TY, int NT, int QP = TX, class Ctx>
 CLAW2_HD void finish_tile(const StepArgs& a, Ctx& ctx, const TileId& tile, const double* Qx, int QSTR, double* red,
-                          double* qout, int i0, int j0, double cflm, double dt)
+                          double* qout, int i0, int j0, double cflm, double dt, bool fault = false)
 {
     const int tid = ctx.tid();
     int bad = 0;
-    for (int idx = tid; idx < TX * TY; idx += NT) {
+    for (int idx = fault ? TX * TY : tid; idx < TX * TY; idx += NT) {
         const int ci = idx % TX, cj = idx / TX;
         const int i = i0 + ci, j = j0 + cj;
         if (i >= a.mx || j >= a.my) continue;
@@ -633,7 +638,8 @@ CLAW2_HD void finish_tile(const StepArgs& a, Ctx& ctx, const TileId& tile, const
 
     // ---- block CFL max (deterministic: max is exact) and last-block epilogue:
     // warp max by shuffles, then one value per warp.  CFL numbers are >= 0; a
-    // NaN one counts as a non-finite state, and -1 flags a warp that saw one.
+    // NaN one counts as a non-finite state, and -1 flags a warp that saw one;
+    // a tile that could not be computed reports -2.
     {
         const bool nfw = ctx.warp_any(bad != 0 || cflm != cflm);
         const double mw = ctx.warp_max(cflm);
@@ -648,7 +654,7 @@ CLAW2_HD void finish_tile(const StepArgs& a, Ctx& ctx, const TileId& tile, const
             if (red[t] < 0.0) nf = 1;
             else mxv = mxv > red[t] ? mxv : red[t];
         }
-        a.partials[tile.part] = nf ? -1.0 : mxv;
+        a.partials[tile.part] = fault ? -2.0 : (nf ? -1.0 : mxv);
         ctx.fence();
         const unsigned int prev = ctx.atomic_inc(a.ticket);
         red[NW] = prev == (unsigned int)(tile.ntiles - 1) ? 1.0 : 0.0;     // this CTA arrived last
@@ -658,22 +664,25 @@ CLAW2_HD void finish_tile(const StepArgs& a, Ctx& ctx, const TileId& tile, const
         // the last CTA reduces every CTA's partial with all its threads
         ctx.fence();
         double cfl = 0.0;
-        bool nonfinite = false;
+        bool nonfinite = false, lost = false;
         for (int b = tid; b < tile.ntiles; b += NT) {
             const double v = ctx.load_volatile(&a.partials[b]);
             if (v < 0.0) nonfinite = true;
             else cfl = cfl > v ? cfl : v;
+            if (v == -2.0) lost = true;
         }
         const bool nfw = ctx.warp_any(nonfinite);
+        const bool lw = ctx.warp_any(lost);
         const double mw = ctx.warp_max(cfl);
-        if ((tid & 31) == 0) red[tid >> 5] = nfw ? -1.0 : mw;
+        if ((tid & 31) == 0) red[tid >> 5] = lw ? -2.0 : (nfw ? -1.0 : mw);
         ctx.sync();
         if (tid == 0) {
             cfl = 0.0;
             int nf = 0;
             for (int t = 0; t < NW; t++) {
-                if (red[t] < 0.0) nf = 1;
-                else cfl = cfl > red[t] ? cfl : red[t];
+                if (red[t] == -2.0) nf = 2;
+                else if (red[t] < 0.0 && nf == 0) nf = 1;
+                else if (red[t] >= 0.0) cfl = cfl > red[t] ? cfl : red[t];
             }
             if (a.ctrl && !a.ctrl_readonly) control_update(a.ctrl, cfl, nf);
             else if (a.ctrl_readonly) *a.cfl_out = nf ? 1.0 / 0.0 : cfl;

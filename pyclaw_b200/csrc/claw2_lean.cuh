@@ -20,18 +20,22 @@
 //    cross-line terms (to the line above and below) go through a
 //    double-buffered shared array: one block barrier per chunk of lines;
 //  - the tile's whole input halo (rows j0-2..j0+TY+1, columns i0-2..i0+TX+1)
-//    is staged in shared memory once, with coalesced row-wise loads all in
-//    flight together; x lines read rows of it and y lines read down its
-//    columns, whose odd pitch keeps those reads free of bank conflicts.
+//    is staged in shared memory once by the tensor memory accelerator (two
+//    boxes of 16 columns x 32 rows x MEQN fields, 128-byte swizzle; see
+//    claw2_tma.cuh) while the threads wait on an mbarrier; x lines read rows
+//    of it and y lines read down its columns.
 #pragma once
 
 #include "claw2_kernels.cuh"
+#include "claw2_tma.cuh"
 
 namespace claw2 {
 
-// Shared memory of the lean body (doubles): the tile state, the cross-line
-// exchange (2 buffers x 2 terms x MEQN x NT), the reduction scratch and the
-// staged input halo (MEQN fields x TR rows x TP columns).
+// Shared memory of the lean body (doubles): the staged input halo (2 boxes x
+// MEQN fields x TR rows x 16 columns, at a 1024-byte boundary for the
+// swizzle), the tile state, the cross-line exchange (2 buffers x 2 terms x
+// MEQN x NT) and the reduction scratch; `bytes` includes up to 1 KB of
+// alignment padding in front of the halo.
 template <class RP, int TX, int TY, int NT> struct LeanSmem {
     static constexpr int MEQN = RP::MEQN;
     static constexpr int QP = TX | 1;            // row pitch of the tile state: odd, so that
@@ -39,30 +43,19 @@ template <class RP, int TX, int TY, int NT> struct LeanSmem {
     static constexpr int QX = MEQN * TY * QP;
     static constexpr int CX = 2 * 2 * MEQN * NT;
     static constexpr int TR = TY + 4;            // rows j0-2 .. j0+TY+1
-    static constexpr int TP = (TX + 4) | 1;      // columns i0-2 .. i0+TX+1, odd pitch
-    static constexpr int HS = MEQN * TR * TP;
-    static constexpr int total = QX + CX + NT + HS;
-    static constexpr int bytes = total * 8;
+    static constexpr int BOX = MEQN * TR * 16;   // one box: columns 16b .. 16b+15 of the halo
+    static constexpr int HS = 2 * BOX;
+    static constexpr int total = HS + QX + CX + NT;
+    static constexpr int bytes = total * 8 + 1024;
+    static_assert(TX + 4 == 32 && TR == 32, "the halo is two 16 x 32 boxes");
+    static_assert((BOX * 8) % 1024 == 0, "each box starts on a 1024-byte boundary");
 };
 
-// Copy the tile's input halo into H: H[(m*TR + r)*TP + c] = q(m, i0-2+c, j0-2+r).
-// Cells outside the ghosted array are set to 0 (no lane reads them).
-template <class RP, int TX, int TY, int NT, class Ctx>
-CLAW2_HD void lean_stage(const StepArgs& a, Ctx& ctx, const double* __restrict__ qin, double* H, int i0, int j0)
+// The staged input of halo row r, column c, field m: H holds q(m, i0-2+c, j0-2+r).
+template <int MEQN, int TR>
+__device__ __forceinline__ int lean_hidx(int m, int r, int c)
 {
-    constexpr int MEQN = RP::MEQN;
-    using SM = LeanSmem<RP, TX, TY, NT>;
-    constexpr int TR = SM::TR, TP = SM::TP, NPOS = TR * TP, FS = TR * TP;
-    const long long P = a.plane;
-    for (int t = ctx.tid(); t < NPOS; t += NT) {
-        const int r = t / TP, c = t - r * TP;
-        const int col = i0 - 2 + c, row = j0 - 2 + r;
-        const bool in = col >= -CLAW2_NUM_GHOST && col < a.mx + CLAW2_NUM_GHOST && row >= -CLAW2_NUM_GHOST &&
-                        row < a.my + CLAW2_NUM_GHOST;
-        const long long o = in ? qoff(a, 0, col, row) : 0;
-#pragma unroll
-        for (int m = 0; m < MEQN; m++) H[m * FS + t] = in ? qin[o + m * P] : 0.0;
-    }
+    return (c >> 4) * (MEQN * TR * 16) + m * (TR * 16) + swz128(r, c & 15);
 }
 
 // One chunk of one sweep direction (arguments as in sweep_chunk); CXb is the
@@ -73,11 +66,11 @@ CLAW2_HD void lean_chunk(const StepArgs& a, Ctx& ctx, const double* H, double* Q
 {
     constexpr int MEQN = RP::MEQN, MW = RP::MW, NROE = RP::NROE;
     using SM = LeanSmem<RP, TX, TY, NT>;
-    constexpr int TR = SM::TR, TP = SM::TP;
+    constexpr int TR = SM::TR;
     // the staged input of cell (kk along the slice, ll across it)
     auto hq = [&](int m, int kk, int ll) -> double {
-        return IXY == 1 ? H[(m * TR + (ll - j0 + 2)) * TP + (kk - i0 + 2)]
-                        : H[(m * TR + (kk - j0 + 2)) * TP + (ll - i0 + 2)];
+        return IXY == 1 ? H[lean_hidx<MEQN, TR>(m, ll - j0 + 2, kk - i0 + 2)]
+                        : H[lean_hidx<MEQN, TR>(m, kk - j0 + 2, ll - i0 + 2)];
     };
     constexpr int NCELL = IXY == 1 ? TX : TY;
     constexpr int NSLOT = NCELL + 3;
@@ -265,37 +258,62 @@ CLAW2_HD void lean_chunk(const StepArgs& a, Ctx& ctx, const double* H, double* Q
 }
 
 // Whole-tile unsplit step with the lean body (the caller checks that the
-// problem has no capacity function and no f-waves).
+// problem has no capacity function and no f-waves).  tm0 / tm1: tensor maps
+// of the input state (uncontrolled mode: both of a.qin; controlled mode: of
+// a.q0 and a.q1) over the ghosted planes (mx+4 x my+4 x MEQN, row pitch ld,
+// 16 x 32 x MEQN boxes, 128-byte swizzle); bar: an mbarrier in shared memory.
+// The halo copy is waited for at most about a second (clock64 cycles); a
+// tile whose copy does not arrive reports a timeout instead of a result.
+constexpr long long kTmaWaitCycles = 2000000000LL;
+
 template <class RP, int TX, int TY, int NT, class Ctx>
-CLAW2_HD void lean_tile_at(const StepArgs& a, Ctx& ctx, const TileId& tile)
+__device__ __forceinline__ void lean_tile_at(const StepArgs& a, Ctx& ctx, const TileId& tile, const CUtensorMap* tm0,
+                                             const CUtensorMap* tm1, uint64_t* bar)
 {
     constexpr int MEQN = RP::MEQN;
     using SM = LeanSmem<RP, TX, TY, NT>;
     constexpr int LPC = NT / 32;
     static_assert(TX + 4 <= 32 && TY + 4 <= 32, "a line's cells i0-2 .. i0+TX+1 must fit its 32 lanes");
     static_assert(RP::MAUX == 0, "the lean body serves the solvers without aux arrays");
-    double* Qx = ctx.smem();
+    double* H = ctx.smem();
+    {
+        const uint32_t s0 = smem_addr(H);
+        H += ((1024u - (s0 & 1023u)) & 1023u) / 8;       // 1024-byte boundary for the swizzled boxes
+    }
+    double* Qx = H + SM::HS;
     double* CX = Qx + SM::QX;
     double* red = CX + SM::CX;
-    double* H = red + NT;
     const int tid = ctx.tid();
     const int warp = tid >> 5;
     const int i0 = tile.bx * TX, j0 = tile.by * TY;
-    const double* qin = a.qin;
     double* qout = a.qout;
     double dt = a.dt;
+    const CUtensorMap* tm = tm0;
     if (a.ctrl) {
         if (a.ctrl->done) return;                  // uniform across the grid
         dt = a.ctrl->dt;
         const int cur = a.ctrl->cur;
-        qin = cur ? a.q1 : a.q0;
+        tm = cur ? tm1 : tm0;
         qout = cur ? a.q0 : a.q1;
+    }
+    // stage the halo: rows j0-2.., columns i0-2.. are ghosted-array indices
+    // j0, i0 (x = i0 is even, so the box starts on a 16-byte boundary)
+    if (tid == 0) {
+        mbar_init(bar, 1);
+        mbar_arrive_expect_tx(bar, (uint32_t)(SM::HS * 8 + a.halo_shortfall));
+        tma_load_3d(H, tm, bar, i0, j0, 0);
+        tma_load_3d(H + SM::BOX, tm, bar, i0 + 16, j0, 0);
     }
     const double dtdx = dt / a.dx, dtdy = dt / a.dy;
     double cflm = 0.0;
     int chunk = 0;
-    lean_stage<RP, TX, TY, NT>(a, ctx, qin, H, i0, j0);
-    ctx.sync();
+    ctx.sync();                                    // the barrier is initialised
+    const bool late = !mbar_wait_bounded(bar, 0, kTmaWaitCycles);
+    if (__syncthreads_or(late)) {                  // the whole CTA takes the same path
+        mbar_wait_bounded(bar, 0, kTmaWaitCycles);  // let a late copy land before the CTA moves on
+        finish_tile<MEQN, TX, TY, NT, SM::QP>(a, ctx, tile, Qx, TY * SM::QP, red, qout, i0, j0, 0.0, dt, true);
+        return;
+    }
     {
         const int first = j0 - 1;
         const int last = (j0 + TY < a.my) ? j0 + TY : a.my;

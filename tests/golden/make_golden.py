@@ -19,7 +19,8 @@ without the reference tree being present:
                             and the fort.t headers (test_acoustics_2d_variable_io.py,
                             reltol 1e-4)
 
-Usage: python tests/golden/make_golden.py [/path/to/reference]
+Usage: python tests/golden/make_golden.py /path/to/reference
+   or: CLAW2_REFERENCE=/path/to/reference python tests/golden/make_golden.py
 """
 import os
 import sys
@@ -65,4 +66,7 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("CLAW2_REFERENCE")
+    if not ref:
+        sys.exit("usage: make_golden.py /path/to/reference  (or set CLAW2_REFERENCE)")
+    main(ref)

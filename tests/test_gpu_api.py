@@ -14,7 +14,7 @@ GOLD = os.path.join(os.path.dirname(__file__), "golden")
 
 
 def _api_run(p, q, aux, run, tfinal, nout, split, trans=2, rp=None, bcs=None, src=None, keep=True,
-             bounds=((0.0, 1.0), (0.0, 1.0)), before_step=None):
+             bounds=((0.0, 1.0), (0.0, 1.0)), before_step=None, outdir=None):
     """Build the same problem through the public API and run it on the GPU."""
     x = pc.Dimension('x', bounds[0][0], bounds[0][1], p.mx)
     y = pc.Dimension('y', bounds[1][0], bounds[1][1], p.my)
@@ -50,6 +50,10 @@ def _api_run(p, q, aux, run, tfinal, nout, split, trans=2, rp=None, bcs=None, sr
     claw.tfinal = tfinal
     claw.num_output_times = nout
     claw.output_format = None
+    if outdir is not None:                      # the app's settings (acoustics.py:71-83)
+        claw.output_format = 'ascii'
+        claw.outdir = outdir
+        claw.write_aux_init = True
     claw.keep_copy = keep
     claw.run()
     return claw, solver
@@ -68,6 +72,33 @@ def test_vc_acoustics_app_matches_golden_and_oracle(orc):
     assert np.max(np.abs(gold - got[0])) < 1e-13
     io = np.load(os.path.join(GOLD, "vc_acoustics_io.npz"))
     assert K.check_diff(io["q20"], got, reltol=1e-4) is None
+
+
+def test_vc_acoustics_app_io_round_trip(tmp_path):
+    """The reference's I/O test (apps/acoustics_2d_variable/
+    test_acoustics_2d_variable_io.py:1-55): the app writes ascii frames through
+    Controller.run while the device runs the steps; frames 0 (with aux) and 20
+    are read back with Solution.read and compared with the reference's
+    io_test_verification files at reltol 1e-4, and the header lines are the
+    reference's text."""
+    p, q, aux, run = K.acoustics_variable_setup()
+    out = str(tmp_path / "_io_test_results")
+    claw, solver = _api_run(p, q, aux, run, 0.6, 20, split=False, trans=1, rp=pc.riemann.rp2_vc_acoustics,
+                            bounds=((-1.0, 1.0), (-1.0, 1.0)), outdir=out)
+    assert sorted(f for f in os.listdir(out) if f.startswith("fort.q")) == ["fort.q%04d" % k for k in range(21)]
+    io = np.load(os.path.join(GOLD, "vc_acoustics_io.npz"))
+    s0 = pc.Solution(0, path=out, file_format='ascii', read_aux=True)
+    s20 = pc.Solution(20, path=out, file_format='ascii', read_aux=False)
+    assert K.check_diff(io["q20"], s20.state.q, reltol=1e-4) is None
+    assert K.check_diff(io["aux0"], s0.state.aux, reltol=1e-4) is None
+    with open(os.path.join(out, "fort.t0020")) as f:
+        assert f.read() == str(io["t_header"])
+    with open(os.path.join(out, "fort.q0020")) as f:
+        assert "\n".join(f.read().splitlines()[:8]) == str(io["q_header"])
+    # what was written is the device's frame at the %18.8e precision
+    dev = claw.frames[20].state.q
+    big = np.abs(dev) > 1e-300
+    assert np.max(np.abs(s20.state.q[big] - dev[big]) / np.abs(dev[big])) <= 5.1e-9
 
 
 def test_acoustics_homogeneous_split_app(orc):

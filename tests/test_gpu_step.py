@@ -182,3 +182,44 @@ def test_repeated_steps_are_deterministic():
     a, ca = H.dev_step(p, qbc, None, 0.002)
     b, cb = H.dev_step(p, qbc, None, 0.002)
     assert ca == cb and np.array_equal(a, b)
+
+
+def test_halo_wait_runs_out_and_reports_timeout(orc):
+    """The TMA-staged lean body waits on an mbarrier for its halo copies with a
+    limit of about a second.  Making every CTA wait for 8 bytes more than its
+    copies deliver (a count that nothing completes) must end the step with
+    CLAW2_ERR_TIMEOUT through the controller, or a NaN CFL number without one,
+    and leave the context usable: the next run is bit-identical to the oracle."""
+    import ctypes
+    import torch
+    from pyclaw_b200 import _abi, _lib
+    from pyclaw_b200.device import DeviceState
+    lib = _lib.load()
+    p = H.problem("euler4", 60, 40, 2, bcl=(1, 3), bcu=(1, 3))
+    q, _ = H.init_fields(p, seed=5)
+
+    def controlled():
+        dev = DeviceState(p)
+        dev.upload_q(q)
+        c = _abi.Control()
+        _lib.check(lib.claw2_control_init(ctypes.byref(c), 0.0, 0.002, 0.01, 1.0, 0.9, 1e99, 1, 0, 100, 0.9),
+                   "claw2_control_init")
+        out = dev.evolve(c)
+        return out, dev.download_q()
+
+    try:
+        _lib.check(lib.claw2_debug_halo_shortfall(8), "claw2_debug_halo_shortfall")
+        out, _ = controlled()
+        assert out.error == _abi.ERR_TIMEOUT and out.numsteps == 0, (out.error, out.numsteps)
+        qbc = orc.new_qbc(p, q)
+        orc.fill_ghosts(p, qbc)
+        _, cfl = H.dev_step(p, qbc, None, 0.002)
+        assert cfl != cfl                       # NaN: the step did not happen
+    finally:
+        lib.claw2_debug_halo_shortfall(0)
+    torch.cuda.synchronize()
+    out, got = controlled()
+    assert out.error == 0 and out.numsteps > 0
+    ref = orc.Run(p, q, None, cfl_max=1.0, cfl_desired=0.9, dt_initial=0.002)
+    ref.evolve_to_time(0.01)
+    assert np.array_equal(got, ref.q) and ref.steps_taken == out.numsteps
