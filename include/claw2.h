@@ -315,7 +315,7 @@ typedef struct claw2_batch_instance {
     int64_t ld, plane;          /* layout of this grid (claw2_get_layout)      */
     int32_t mx, my;
     double dx, dy;
-    int32_t nbx, nby;           /* tiles (claw2_batch_tiles)                   */
+    int32_t nbx, nby;           /* tiles (claw2_batch_tiles_for the variant's edge) */
     int32_t tile_begin;         /* index of this instance's first tile         */
     int32_t pad_;
 } claw2_batch_instance;
@@ -324,7 +324,12 @@ typedef struct claw2_batch_instance {
 CLAW2_EXPORT int claw2_batch_num_variants(void);
 /* Threads per CTA and resident CTAs per SM of variant v (for reporting). */
 CLAW2_EXPORT int claw2_batch_variant_info(int v, int* threads, int* ctas_per_sm);
-/* Tiles of an mx x my instance. */
+/* Tile edge (cells) of variant v: 29, 21 or 13; -1 for an invalid v.  The
+ * descriptors passed with variant v must number the tiles of that edge. */
+CLAW2_EXPORT int claw2_batch_variant_tile(int v);
+/* Tiles of an mx x my instance for a tile edge of 29, 21 or 13 cells. */
+CLAW2_EXPORT int claw2_batch_tiles_for(int tile, int mx, int my, int* nbx, int* nby);
+/* Tiles of an mx x my instance with 29x29 tiles (variants 0-5). */
 CLAW2_EXPORT int claw2_batch_tiles(int mx, int my, int* nbx, int* nby);
 /* nsteps launches of the batched step: every launch takes one controlled step
  * (Solver.evolve_to_time's loop body, src/pyclaw/solver.py:632-691) of every

@@ -49,6 +49,9 @@ PROTOTYPES = [
                                                 ctypes.POINTER(ctypes.c_int)]),
     ("claw2_batch_tiles", ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
                                          ctypes.POINTER(ctypes.c_int)]),
+    ("claw2_batch_variant_tile", ctypes.c_int, [ctypes.c_int]),
+    ("claw2_batch_tiles_for", ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                             ctypes.POINTER(ctypes.c_int)]),
     ("claw2_batch_advance", ctypes.c_int, [_P, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp]),
     ("claw2_batch_graph_create", ctypes.c_int, [_P, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                                 ctypes.POINTER(_vp)]),

@@ -4,8 +4,9 @@ Every instance has its own grid size, spacing, aux fields and time-step
 controller (its own dt from its own CFL number).  One launch of the batched
 kernel takes one controlled step of every instance; the run of launches is
 captured once into a CUDA graph and replayed.  The launch configuration
-(threads per CTA and CTAs per SM of the persistent grid) is chosen by
-`autotune`, which times the candidates on the actual batch.
+(threads per CTA, CTAs per SM of the persistent grid, and the tile edge, i.e.
+the cells a CTA takes per work item) is chosen by `autotune`, which times the
+candidates on the actual batch.
 
 The reference steps one patch per call (ClawSolver2D.step_hyperbolic,
 src/pyclaw/classic/solver.py:498-547); each instance here follows exactly that
@@ -59,11 +60,17 @@ class BatchSolver(object):
         self.device = torch.device(device if device is not None else "cuda")
         self.cfl_max, self.cfl_desired, self.dt_max = cfl_max, cfl_desired, dt_max
         meqn, maux = problem.num_eqn, problem.num_aux
-        descs = (BatchInstance * self.n)()
+        nv = self.lib.claw2_batch_num_variants()
+        self.tile_of = {v: self.lib.claw2_batch_variant_tile(v) for v in range(nv)}
+        edges = sorted(set(self.tile_of.values()), reverse=True)
+        # one descriptor table per tile edge: the tiles of every instance
+        # numbered consecutively; partials sized for the smallest edge
+        tables = {e: (BatchInstance * self.n)() for e in edges}
         self.layouts = []
         self.problems = []
         offs_q, offs_a, offs_p = [], [], []
-        nq = na = npart = ntiles = 0
+        nq = na = npart = 0
+        ntiles = {e: 0 for e in edges}
         for k, inst in enumerate(instances):
             q = inst["q"]
             mx, my = q.shape[1], q.shape[2]
@@ -71,8 +78,6 @@ class BatchSolver(object):
             pk.mx, pk.my, pk.dx, pk.dy = mx, my, float(inst["dx"]), float(inst["dy"])
             _lib.check(self.lib.claw2_validate(ctypes.byref(pk)), "claw2_validate (instance %d)" % k)
             L = _lib.layout(pk)
-            nbx, nby = ctypes.c_int(), ctypes.c_int()
-            _lib.check(self.lib.claw2_batch_tiles(mx, my, ctypes.byref(nbx), ctypes.byref(nby)), "claw2_batch_tiles")
             self.layouts.append(L)
             self.problems.append(pk)
             offs_q.append(nq)
@@ -80,12 +85,19 @@ class BatchSolver(object):
             offs_a.append(na)
             na += L.aux_elems
             offs_p.append(npart)
-            npart += nbx.value * nby.value
-            d = descs[k]
-            d.ld, d.plane, d.mx, d.my, d.dx, d.dy = L.ld, L.plane, mx, my, pk.dx, pk.dy
-            d.nbx, d.nby, d.tile_begin = nbx.value, nby.value, ntiles
-            ntiles += nbx.value * nby.value
-        self.ntiles = ntiles
+            most = 0
+            for e in edges:
+                nbx, nby = ctypes.c_int(), ctypes.c_int()
+                _lib.check(self.lib.claw2_batch_tiles_for(e, mx, my, ctypes.byref(nbx), ctypes.byref(nby)),
+                           "claw2_batch_tiles_for")
+                d = tables[e][k]
+                d.ld, d.plane, d.mx, d.my, d.dx, d.dy = L.ld, L.plane, mx, my, pk.dx, pk.dy
+                d.nbx, d.nby, d.tile_begin = nbx.value, nby.value, ntiles[e]
+                ntiles[e] += nbx.value * nby.value
+                most = max(most, nbx.value * nby.value)
+            npart += most
+        self.ntiles_of = ntiles
+        self.ntiles = ntiles[29]
         f64 = dict(dtype=torch.float64, device=self.device)
         self.qarena = torch.zeros(max(nq, 1), **f64)
         self.aarena = torch.zeros(max(na, 1), **f64)
@@ -95,17 +107,20 @@ class BatchSolver(object):
         self.ctrl = torch.zeros(self.n * csz, dtype=torch.uint8, device=self.device)
         self.ctrl_host = torch.zeros(self.n * csz, dtype=torch.uint8).pin_memory()
         base_q, base_a = self.qarena.data_ptr(), self.aarena.data_ptr()
-        for k in range(self.n):
-            d, L = descs[k], self.layouts[k]
-            d.q0 = base_q + 8 * offs_q[k]
-            d.q1 = base_q + 8 * (offs_q[k] + L.q_elems)
-            d.aux = (base_a + 8 * offs_a[k]) if maux > 0 else None
-            d.ctrl = self.ctrl.data_ptr() + k * csz
-            d.partials = self.partials.data_ptr() + 8 * offs_p[k]
-            d.ticket = self.tickets.data_ptr() + 4 * k
-        self.descs = descs
+        for descs in tables.values():
+            for k in range(self.n):
+                d, L = descs[k], self.layouts[k]
+                d.q0 = base_q + 8 * offs_q[k]
+                d.q1 = base_q + 8 * (offs_q[k] + L.q_elems)
+                d.aux = (base_a + 8 * offs_a[k]) if maux > 0 else None
+                d.ctrl = self.ctrl.data_ptr() + k * csz
+                d.partials = self.partials.data_ptr() + 8 * offs_p[k]
+                d.ticket = self.tickets.data_ptr() + 4 * k
+        self.descs = tables[29]
         self.offs_q, self.offs_a = offs_q, offs_a
-        self.desc_dev = torch.frombuffer(bytearray(bytes(descs)), dtype=torch.uint8).to(self.device)
+        self.desc_dev_of = {e: torch.frombuffer(bytearray(bytes(t)), dtype=torch.uint8).to(self.device)
+                            for e, t in tables.items()}
+        self.desc_dev = self.desc_dev_of[29]
         self.variant = 0
         self._graphs = {}
         self.tuning = None
@@ -164,11 +179,17 @@ class BatchSolver(object):
     def _stream(self):
         return ctypes.c_void_p(self.torch.cuda.current_stream(self.device).cuda_stream)
 
+    def _table(self, v):
+        """(device descriptor table, tile count) numbering the tiles of variant v's edge."""
+        e = self.tile_of[v]
+        return self.desc_dev_of[e], self.ntiles_of[e]
+
     def advance(self, nsteps, variant=None):
         """nsteps batched launches (no graph)."""
         v = self.variant if variant is None else variant
-        _lib.check(self.lib.claw2_batch_advance(ctypes.byref(self.p), ctypes.c_void_p(self.desc_dev.data_ptr()),
-                                                self.n, self.ntiles, int(nsteps), int(v), self._stream()),
+        desc, nt = self._table(v)
+        _lib.check(self.lib.claw2_batch_advance(ctypes.byref(self.p), ctypes.c_void_p(desc.data_ptr()),
+                                                self.n, nt, int(nsteps), int(v), self._stream()),
                    "claw2_batch_advance")
 
     def advance_graph(self, nsteps, chunk=50):
@@ -180,9 +201,9 @@ class BatchSolver(object):
             key = (count, self.variant)
             if key not in self._graphs:
                 ge = ctypes.c_void_p()
-                _lib.check(self.lib.claw2_batch_graph_create(ctypes.byref(self.p),
-                                                             ctypes.c_void_p(self.desc_dev.data_ptr()), self.n,
-                                                             self.ntiles, count, self.variant, ctypes.byref(ge)),
+                desc, nt = self._table(self.variant)
+                _lib.check(self.lib.claw2_batch_graph_create(ctypes.byref(self.p), ctypes.c_void_p(desc.data_ptr()),
+                                                             self.n, nt, count, self.variant, ctypes.byref(ge)),
                            "claw2_batch_graph_create")
                 self._graphs[key] = ge
             for _ in range(reps):
@@ -215,12 +236,14 @@ class BatchSolver(object):
                 best = min(best, e0.elapsed_time(e1) / steps)
             th, cps = ctypes.c_int(), ctypes.c_int()
             self.lib.claw2_batch_variant_info(v, ctypes.byref(th), ctypes.byref(cps))
-            times[v] = {"ms_per_launch": best, "threads": th.value, "ctas_per_sm": cps.value}
+            times[v] = {"ms_per_launch": best, "threads": th.value, "ctas_per_sm": cps.value,
+                        "tile": self.tile_of[v], "tiles": self._table(v)[1]}
         self.qarena.copy_(q_save)
         self.ctrl.copy_(c_save)
         self.tickets.zero_()
         torch.cuda.synchronize(self.device)
         self.variant = min(times, key=lambda v: times[v]["ms_per_launch"])
+        self.desc_dev, self.ntiles = self._table(self.variant)
         self.tuning = {"chosen": self.variant, "candidates": times}
         return self.tuning
 

@@ -138,19 +138,20 @@ __device__ __forceinline__ int batch_prefetch_tile(const claw2_batch_instance* _
 }
 
 // Batched step: a persistent grid walks the concatenated tile list of all
-// instances; each tile is one step_tile_at call with that instance's buffers,
-// with an L2 prefetch of the CTA's next tile issued first.
-template <class RP, int NT, int MINB, bool LIGHT>
+// instances; each tile (T x T cells) is one tile-body call with that
+// instance's buffers, with an L2 prefetch of the CTA's next tile issued first.
+template <class RP, int NT, int MINB, bool LIGHT, int T>
 __global__ void __launch_bounds__(NT, MINB)
 batch_kernel(const claw2_batch_instance* __restrict__ inst, int ninst, int ntiles, StepArgs common)
 {
+    static_assert(LIGHT || T == 29, "the generic body runs 29x29 tiles in the batch");
     extern __shared__ double smem_dyn[];
     DevCtx ctx{smem_dyn};
     int next = -1;                                  // instance of the next tile, found by its prefetch
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
         const int lo = next >= 0 ? next : batch_instance_of(inst, ninst, t);
         next = t + (int)gridDim.x < ntiles
-                   ? batch_prefetch_tile<RP::MEQN, RP::MAUX, 29, 29, NT>(inst, ninst, t + (int)gridDim.x)
+                   ? batch_prefetch_tile<RP::MEQN, RP::MAUX, T, T, NT>(inst, ninst, t + (int)gridDim.x)
                    : -1;
         const claw2_batch_instance& I = inst[lo];
         StepArgs a = common;
@@ -160,7 +161,7 @@ batch_kernel(const claw2_batch_instance* __restrict__ inst, int ninst, int ntile
         a.ghost_fused = (I.mx >= 4 && I.my >= 4) ? common.ghost_fused : 0;
         const int lt = t - I.tile_begin;
         const TileId tile{lt % I.nbx, lt / I.nbx, I.nbx, I.nby, lt, I.nbx * I.nby};
-        if constexpr (LIGHT) light_tile_at<RP, 29, 29, NT>(a, ctx, tile);
+        if constexpr (LIGHT) light_tile_at<RP, T, T, NT>(a, ctx, tile);
         else step_tile_at<RP, 29, 29, NT, false>(a, ctx, tile);
         __syncthreads();                            // shared memory is reused by the next tile
     }
@@ -782,18 +783,25 @@ int claw2_device_to_ref(const claw2_problem* p, int ncomp, const double* dev, do
 }  // extern "C"
 
 namespace {
-struct BatchVariant { int threads, minb; };
-// the last two exist for the light body only (claw2_batch_advance returns
-// CLAW2_ERR_UNSUPPORTED for them with the other solvers)
-constexpr BatchVariant kBatchVariants[] = {{256, 2}, {128, 4}, {128, 3}, {512, 1}, {256, 3}, {256, 4}};
+// threads per CTA, resident CTAs per SM, tile edge (cells per CTA per work
+// item = tile^2).  Variants 4.. exist for the light acoustics body only
+// (claw2_batch_advance returns CLAW2_ERR_UNSUPPORTED for them with the other
+// solvers); a line of the light body has 32 lanes for tile + 3 interfaces, so
+// smaller tiles leave lanes idle but waste fewer cells at instance edges.
+struct BatchVariant { int threads, minb, tile; };
+constexpr BatchVariant kBatchVariants[] = {{256, 2, 29}, {128, 4, 29}, {128, 3, 29}, {512, 1, 29},
+                                           {256, 3, 29}, {256, 4, 29}, {256, 3, 21}, {256, 4, 21},
+                                           {256, 3, 13}, {256, 4, 13}};
 constexpr int kNumBatchVariants = sizeof(kBatchVariants) / sizeof(kBatchVariants[0]);
 
-template <class RP, int NT, int MINB, bool LIGHT>
+bool batch_tile_ok(int tile) { return tile == 29 || tile == 21 || tile == 13; }
+
+template <class RP, int NT, int MINB, bool LIGHT, int T>
 int batch_launch_t(const StepArgs& common, const claw2_batch_instance* inst, int ninst, int ntiles, int nsteps,
                    cudaStream_t st)
 {
-    constexpr int SMB = LIGHT ? LightSmem<29, 29, NT>::bytes : TileSmem<RP, 29, 29, NT, false>::bytes;
-    auto kern = batch_kernel<RP, NT, MINB, LIGHT>;
+    constexpr int SMB = LIGHT ? LightSmem<T, T, NT>::bytes : TileSmem<RP, 29, 29, NT, false>::bytes;
+    auto kern = batch_kernel<RP, NT, MINB, LIGHT, T>;
     static std::atomic<uint64_t> optin{0};
     static std::atomic<int> grids[kDevAttrSlots];
     const int grid = persistent_grid(optin, grids, kern, NT, SMB);
@@ -813,23 +821,26 @@ int batch_launch_rp(int variant, const StepArgs& c, const claw2_batch_instance* 
     if constexpr (HasLight<RP>::value) {
         if (c.capa < 0 && !c.fwave) {
             switch (variant) {
-            case 0: return batch_launch_t<RP, 256, 2, true>(c, inst, ninst, ntiles, nsteps, st);
-            case 1: return batch_launch_t<RP, 128, 4, true>(c, inst, ninst, ntiles, nsteps, st);
-            case 2: return batch_launch_t<RP, 128, 3, true>(c, inst, ninst, ntiles, nsteps, st);
-            case 3: return batch_launch_t<RP, 512, 1, true>(c, inst, ninst, ntiles, nsteps, st);
-            case 4: return batch_launch_t<RP, 256, 3, true>(c, inst, ninst, ntiles, nsteps, st);
-            case 5: return batch_launch_t<RP, 256, 4, true>(c, inst, ninst, ntiles, nsteps, st);
+            case 0: return batch_launch_t<RP, 256, 2, true, 29>(c, inst, ninst, ntiles, nsteps, st);
+            case 1: return batch_launch_t<RP, 128, 4, true, 29>(c, inst, ninst, ntiles, nsteps, st);
+            case 2: return batch_launch_t<RP, 128, 3, true, 29>(c, inst, ninst, ntiles, nsteps, st);
+            case 3: return batch_launch_t<RP, 512, 1, true, 29>(c, inst, ninst, ntiles, nsteps, st);
+            case 4: return batch_launch_t<RP, 256, 3, true, 29>(c, inst, ninst, ntiles, nsteps, st);
+            case 5: return batch_launch_t<RP, 256, 4, true, 29>(c, inst, ninst, ntiles, nsteps, st);
+            case 6: return batch_launch_t<RP, 256, 3, true, 21>(c, inst, ninst, ntiles, nsteps, st);
+            case 7: return batch_launch_t<RP, 256, 4, true, 21>(c, inst, ninst, ntiles, nsteps, st);
+            case 8: return batch_launch_t<RP, 256, 3, true, 13>(c, inst, ninst, ntiles, nsteps, st);
+            case 9: return batch_launch_t<RP, 256, 4, true, 13>(c, inst, ninst, ntiles, nsteps, st);
             default: return CLAW2_ERR_INVALID;
             }
         }
     }
     switch (variant) {
-    case 0: return batch_launch_t<RP, 256, 2, false>(c, inst, ninst, ntiles, nsteps, st);
-    case 1: return batch_launch_t<RP, 128, 4, false>(c, inst, ninst, ntiles, nsteps, st);
-    case 2: return batch_launch_t<RP, 128, 3, false>(c, inst, ninst, ntiles, nsteps, st);
-    case 3: return batch_launch_t<RP, 512, 1, false>(c, inst, ninst, ntiles, nsteps, st);
-    case 4: case 5: return CLAW2_ERR_UNSUPPORTED;
-    default: return CLAW2_ERR_INVALID;
+    case 0: return batch_launch_t<RP, 256, 2, false, 29>(c, inst, ninst, ntiles, nsteps, st);
+    case 1: return batch_launch_t<RP, 128, 4, false, 29>(c, inst, ninst, ntiles, nsteps, st);
+    case 2: return batch_launch_t<RP, 128, 3, false, 29>(c, inst, ninst, ntiles, nsteps, st);
+    case 3: return batch_launch_t<RP, 512, 1, false, 29>(c, inst, ninst, ntiles, nsteps, st);
+    default: return variant < kNumBatchVariants ? CLAW2_ERR_UNSUPPORTED : CLAW2_ERR_INVALID;
     }
 }
 
@@ -881,9 +892,20 @@ int claw2_batch_variant_info(int v, int* threads, int* ctas_per_sm)
 
 int claw2_batch_tiles(int mx, int my, int* nbx, int* nby)
 {
-    if (mx < 4 || my < 4 || !nbx || !nby) return CLAW2_ERR_INVALID;
-    *nbx = (mx + UTX - 1) / UTX;
-    *nby = (my + UTY - 1) / UTY;
+    return claw2_batch_tiles_for(UTX, mx, my, nbx, nby);
+}
+
+int claw2_batch_variant_tile(int v)
+{
+    if (v < 0 || v >= kNumBatchVariants) return -1;
+    return kBatchVariants[v].tile;
+}
+
+int claw2_batch_tiles_for(int tile, int mx, int my, int* nbx, int* nby)
+{
+    if (!batch_tile_ok(tile) || mx < 4 || my < 4 || !nbx || !nby) return CLAW2_ERR_INVALID;
+    *nbx = (mx + tile - 1) / tile;
+    *nby = (my + tile - 1) / tile;
     return CLAW2_OK;
 }
 
