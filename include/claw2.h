@@ -247,6 +247,34 @@ CLAW2_EXPORT int claw2_advance_hooked(const claw2_problem* p, double* q0, double
                                       claw2_control* ctrl, void* scratch, int nsteps, const claw2_hooks* hooks,
                                       void* stream);
 
+/* ---- gauges recorded on the device ---------------------------------- */
+/* Solver.write_gauge_values (src/pyclaw/solver.py:713-742) samples q at every
+ * gauge cell after each accepted step (evolve_to_time, solver.py:654-656) and
+ * hands it to compute_gauge_values on the host.  A recorder keeps those
+ * samples on the device instead, so the time loop stays on the GPU: after a
+ * step accepted by the controller, record row r = state[0] gets, for gauge k,
+ * record[(r*ngauges + k)*(1+num_eqn) + 0] = t and [.. + 1 + m] = q(m, ix, iy)
+ * of the new state, and state[0] grows by one.  The caller drains the rows
+ * and sets state[0] back to 0 before `capacity` rows are full; a step
+ * accepted with no free row sets state[2] = 1 and is not recorded.  A gauge
+ * cell outside 0 <= ix < mx, 0 <= iy < my records NaN.  All pointers are
+ * device memory. */
+typedef struct claw2_gauges {
+    int32_t ngauges;
+    int32_t capacity;            /* rows of `record`                             */
+    const int32_t* cells;        /* ngauges pairs (ix, iy) of interior cells     */
+    double* record;              /* capacity x ngauges x (1 + num_eqn) doubles    */
+    int64_t* state;              /* [0] rows written, [1] numsteps of the last
+                                    row (set it to ctrl->numsteps at the start),
+                                    [2] overflow flag                            */
+} claw2_gauges;
+
+/* claw2_advance (with the source term of `hooks` when hooks is not NULL) and
+ * the gauge recorder `g` run after every step. */
+CLAW2_EXPORT int claw2_advance_gauged(const claw2_problem* p, double* q0, double* q1, const double* aux,
+                                      claw2_control* ctrl, void* scratch, int nsteps, const claw2_hooks* hooks,
+                                      const claw2_gauges* g, void* stream);
+
 /* ---- domain decomposition: one slab of a larger grid per process -------- */
 /* The reference runs one grid per process under PETSc (PetClaw: a DA with a
  * halo exchange, src/petclaw/state.py:268, and a global CFL max,

@@ -77,6 +77,17 @@ class Hooks(ctypes.Structure):
     ]
 
 
+class Gauges(ctypes.Structure):
+    """struct claw2_gauges (device pointers)."""
+    _fields_ = [
+        ("ngauges", ctypes.c_int32),
+        ("capacity", ctypes.c_int32),
+        ("cells", ctypes.c_void_p),
+        ("record", ctypes.c_void_p),
+        ("state", ctypes.c_void_p),
+    ]
+
+
 class Layout(ctypes.Structure):
     """struct claw2_layout."""
     _fields_ = [

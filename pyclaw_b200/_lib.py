@@ -35,6 +35,8 @@ PROTOTYPES = [
     ("claw2_advance", ctypes.c_int, [_P, _dp, _dp, _dp, _vp, _vp, ctypes.c_int, _vp]),
     ("claw2_advance_hooked", ctypes.c_int, [_P, _dp, _dp, _dp, _vp, _vp, ctypes.c_int, ctypes.POINTER(_abi.Hooks),
                                             _vp]),
+    ("claw2_advance_gauged", ctypes.c_int, [_P, _dp, _dp, _dp, _vp, _vp, ctypes.c_int, ctypes.POINTER(_abi.Hooks),
+                                            ctypes.POINTER(_abi.Gauges), _vp]),
     ("claw2_step_ctrl", ctypes.c_int, [_P, _dp, _dp, _dp, _vp, _vp, _dp, _vp]),
     ("claw2_control_apply", ctypes.c_int, [_vp, _dp, _vp]),
     ("claw2_fill_ghosts_ctrl", ctypes.c_int, [_P, _dp, _dp, _vp, _vp]),

@@ -5,8 +5,10 @@ ClawSolver2D keeps the reference's attributes and call contract
 stays in GPU memory and the step is the fused sm_100a kernel of libclaw2.so.
 evolve_to_time runs the whole step-size control loop on the device (one kernel
 launch per step, no host round trip) unless a Python callback (before_step,
-step_source, a custom boundary condition, gauges) has to run between steps;
-the callbacks of pyclaw_b200.hooks run on the device.
+step_source, a custom boundary condition) has to run between steps; the
+callbacks of pyclaw_b200.hooks run on the device, and gauges are sampled on
+the device after every accepted step and written out after each batch of
+steps.
 """
 import ctypes
 import warnings
@@ -231,8 +233,7 @@ class ClawSolver2D(ClawSolver):
         return h
 
     def _device_loop_ok(self, solution):
-        return (self.before_step is None and self._device_hooks() is not None
-                and len(solution.state.grid.gauges) == 0)
+        return self.before_step is None and self._device_hooks() is not None
 
     def evolve_to_time(self, solution, tend=None):
         if not self._is_set_up:
@@ -266,7 +267,16 @@ class ClawSolver2D(ClawSolver):
                                     self.user_bc_upper, negate=True)
                 dev.set_ghosted_ref(qbc, dev.cur)
                 dev.set_ghosted_ref(qbc, 1 - dev.cur)
-        out = self._dev.evolve(c, hooks=hooks)
+        gauges = [(int(g[0]), int(g[1])) for g in state.grid.gauges]
+        on_gauges = None
+        if gauges:
+            # write_gauge_values after every accepted step (solver.py:654-656),
+            # from samples the device recorded step by step
+            def on_gauges(rows):
+                for r in range(rows.shape[0]):
+                    for i in range(len(gauges)):
+                        self._write_gauge_sample(state, i, float(rows[r, i, 0]), rows[r, i, 1:])
+        out = self._dev.evolve(c, hooks=hooks, gauges=gauges or None, on_gauges=on_gauges)
         solution.t = out.t
         self.dt = out.dt
         self.cfl.update_global_max(out.cfl)

@@ -296,6 +296,41 @@ __global__ void halo_kernel(double* q0, double* q1, const claw2_control* c, doub
     }
 }
 
+// Gauge samples after a step (claw2_gauges): one block; nothing happens
+// unless the controller accepted a step since the last row.
+__global__ void gauge_record_kernel(claw2_gauges g, const double* q0, const double* q1, const claw2_control* c,
+                                    int meqn, long long ld, long long plane, int mx, int my)
+{
+    __shared__ int row;
+    if (threadIdx.x == 0) {
+        row = -1;
+        if (c->numsteps != g.state[1]) {
+            if (g.state[0] < g.capacity) row = (int)g.state[0];
+            else g.state[2] = 1;
+        }
+    }
+    __syncthreads();
+    if (row < 0) return;
+    const double* q = c->cur ? q1 : q0;
+    const int w = 1 + meqn;
+    for (int idx = threadIdx.x; idx < g.ngauges * w; idx += blockDim.x) {
+        const int k = idx / w, m = idx - k * w;
+        double v;
+        if (m == 0) v = c->t;
+        else {
+            const int ix = g.cells[2 * k], iy = g.cells[2 * k + 1];
+            if (ix < 0 || ix >= mx || iy < 0 || iy >= my) v = __longlong_as_double(0x7ff8000000000000ULL);
+            else v = q[(long long)(m - 1) * plane + (long long)(iy + CLAW2_NUM_GHOST) * ld + ix + CLAW2_NUM_GHOST];
+        }
+        g.record[((long long)row * g.ngauges + k) * w + m] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        g.state[0] = row + 1;
+        g.state[1] = c->numsteps;
+    }
+}
+
 }  // namespace claw2
 
 using namespace claw2;
@@ -675,6 +710,39 @@ int claw2_advance_hooked(const claw2_problem* p, double* q0, double* q1, const d
         if (!a.ghost_fused &&
             (rc = launch_fill(p, nullptr, p->num_eqn, p->bc_lower, p->bc_upper, false, q0, q1, ctrl, S(stream))))
             return rc;
+    }
+    return CLAW2_OK;
+}
+
+int claw2_advance_gauged(const claw2_problem* p, double* q0, double* q1, const double* aux, claw2_control* ctrl,
+                         void* scratch, int nsteps, const claw2_hooks* hooks, const claw2_gauges* g, void* stream)
+{
+    int rc = claw2_validate(p);
+    if (rc) return rc;
+    if (!q0 || !q1 || !ctrl || !scratch || !g || (p->num_aux > 0 && !aux) || nsteps < 0) return CLAW2_ERR_INVALID;
+    if (g->ngauges < 1 || g->capacity < 1 || !g->cells || !g->record || !g->state) return CLAW2_ERR_INVALID;
+    StepArgs a;
+    fill_args(p, q0, a);
+    a.q0 = q0; a.q1 = q1; a.aux = aux; a.ctrl = ctrl;
+    a.ticket = static_cast<unsigned int*>(scratch);
+    a.partials = reinterpret_cast<double*>(static_cast<char*>(scratch) + 64);
+    if (hooks) {
+        if (hooks->source != CLAW2_SRC_NONE && hooks->source != CLAW2_SRC_EULER_RADIAL) return CLAW2_ERR_INVALID;
+        if (hooks->source == CLAW2_SRC_EULER_RADIAL &&
+            ((p->rp != CLAW2_RP_EULER_4WAVE && p->rp != CLAW2_RP_EULER_5WAVE) || hooks->source_aux < 0 ||
+             hooks->source_aux >= p->num_aux))
+            return CLAW2_ERR_UNSUPPORTED;
+        a.src = hooks->source;
+        a.src_aux = hooks->source_aux;
+    }
+    const int threads = 128;
+    for (int n = 0; n < nsteps; n++) {
+        if ((rc = launch_step(p, a, S(stream)))) return rc;
+        if (!a.ghost_fused &&
+            (rc = launch_fill(p, nullptr, p->num_eqn, p->bc_lower, p->bc_upper, false, q0, q1, ctrl, S(stream))))
+            return rc;
+        gauge_record_kernel<<<1, threads, 0, S(stream)>>>(*g, q0, q1, ctrl, p->num_eqn, a.ld, a.plane, p->mx, p->my);
+        if (cudaGetLastError() != cudaSuccess) return CLAW2_ERR_CUDA;
     }
     return CLAW2_OK;
 }

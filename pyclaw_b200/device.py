@@ -114,6 +114,14 @@ class DeviceState(object):
             self.host_dirty = False
             self.device_newer = False
 
+    def cells_q(self, cells):
+        """q(:, ix, iy) of the current state at the interior cells `cells`,
+        gathered on the device (one small copy instead of the whole field)."""
+        torch = _torch()
+        ix = torch.tensor([c[0] for c in cells], dtype=torch.long, device=self.device)
+        iy = torch.tensor([c[1] for c in cells], dtype=torch.long, device=self.device)
+        return self.interior(self.cur)[:, iy, ix].cpu().numpy()
+
     def ghosted_ref(self):
         """Current q with ghost cells, in the reference layout (num_eqn, mx+4, my+4), on the host."""
         v = self.qview(self.cur)[:, :, :self.p.mx + 2 * _abi.NUM_GHOST].permute(0, 2, 1).cpu().numpy()
@@ -135,18 +143,53 @@ class DeviceState(object):
         cfl = float(self.cfl_dev.item())
         return cfl, nxt
 
-    def evolve(self, control, max_batch=64, hooks=None):
+    def gauge_recorder(self, cells, capacity):
+        """Device buffers of a claw2_gauges recorder for the interior cells
+        `cells` [(ix, iy), ...]; rows are drained by evolve()."""
+        torch = _torch()
+        g = _abi.Gauges()
+        n = len(cells)
+        self._g_cells = torch.tensor([c for xy in cells for c in xy], dtype=torch.int32, device=self.device)
+        self._g_record = torch.zeros(capacity * n * (1 + self.p.num_eqn), dtype=torch.float64, device=self.device)
+        self._g_state = torch.zeros(3, dtype=torch.int64, device=self.device)
+        g.ngauges, g.capacity = n, capacity
+        g.cells, g.record, g.state = (self._g_cells.data_ptr(), self._g_record.data_ptr(), self._g_state.data_ptr())
+        return g
+
+    def evolve(self, control, max_batch=64, hooks=None, gauges=None, on_gauges=None):
         """Run the device-controlled loop until control is done; returns the
-        final Control.  hooks: a claw2_hooks (source term run on the device)."""
+        final Control.  hooks: a claw2_hooks (source term run on the device).
+        gauges: a list of interior cells (ix, iy) sampled after every accepted
+        step on the device; on_gauges(rows) gets the samples after every batch
+        of steps, rows[r, k] = (t, q(:, ix_k, iy_k)) in step order."""
         torch = _torch()
         control.cur = self.cur
         host = _abi.Control.from_address(self.ctrl_host.data_ptr())
         ctypes.memmove(ctypes.addressof(host), ctypes.addressof(control), ctypes.sizeof(control))
         self.ctrl.copy_(self.ctrl_host, non_blocking=True)
         stream = torch.cuda.current_stream(self.device)
+        rec = None
+        if gauges:
+            rec = self.gauge_recorder(gauges, max_batch)
+            self._g_state[1] = int(control.numsteps)
         batch = 8
         while True:
-            if hooks is None:
+            if rec is not None:
+                _lib.check(self.lib.claw2_advance_gauged(ctypes.byref(self.p), self.ptr(self.q[0]),
+                                                         self.ptr(self.q[1]), self.ptr(self.aux), self.ptr(self.ctrl),
+                                                         self.ptr(self.scratch), int(batch),
+                                                         ctypes.byref(hooks) if hooks is not None else None,
+                                                         ctypes.byref(rec), self.stream), "claw2_advance_gauged")
+                st = self._g_state.cpu()             # waits for the batch
+                nrows = int(st[0])
+                if int(st[2]):
+                    raise RuntimeError("gauge recorder overflow")
+                if nrows:
+                    rows = self._g_record[:nrows * len(gauges) * (1 + self.p.num_eqn)].cpu().numpy()
+                    self._g_state[0] = 0
+                    if on_gauges is not None:
+                        on_gauges(rows.reshape(nrows, len(gauges), 1 + self.p.num_eqn))
+            elif hooks is None:
                 _lib.check(self.lib.claw2_advance(ctypes.byref(self.p), self.ptr(self.q[0]), self.ptr(self.q[1]),
                                                   self.ptr(self.aux), self.ptr(self.ctrl), self.ptr(self.scratch),
                                                   int(batch), self.stream), "claw2_advance")

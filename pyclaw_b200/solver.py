@@ -217,21 +217,33 @@ class Solver(object):
     # ---- gauges (solver.py:713-742) ----------------------------------------
     def write_gauge_values(self, solution):
         state = solution.state
-        for i, gauge in enumerate(state.grid.gauges):
-            ix, iy = gauge[0], gauge[1]
-            q = state.get_q_host()[:, ix, iy]
-            aux = state.aux[:, ix, iy] if state.num_aux > 0 else None
-            p = self.compute_gauge_values(q, aux)
-            t = solution.t
-            if state.keep_gauges:
-                gauge_data = state.gauge_data
-                if len(gauge_data) == len(state.grid.gauges):
-                    gauge_data[i] = np.vstack((gauge_data[i], np.append(t, p)))
-                else:
-                    gauge_data.append(np.append(t, p))
-            try:
-                state.grid.gauge_files[i].write(str(t) + ' ' + ' '.join(str(j) for j in p) + '\n')
-            except Exception:
-                raise Exception("Gauge files are not set up correctly. You should call the method "
-                                "`setup_gauge_files` of the Grid class object before any call for "
-                                "`write_gauge_values` from the Solver class.")
+        gauges = state.grid.gauges
+        if not gauges:
+            return
+        dev = state._dev
+        if dev is not None and dev.device_newer:
+            qs = dev.cells_q(gauges)          # only the gauge cells leave the device
+        else:
+            qh = state.get_q_host()
+            qs = np.stack([qh[:, g[0], g[1]] for g in gauges], axis=1)
+        for i in range(len(gauges)):
+            self._write_gauge_sample(state, i, solution.t, qs[:, i])
+
+    def _write_gauge_sample(self, state, i, t, q):
+        """One gauge's sample at time t: compute_gauge_values on q and the
+        gauge cell's aux, kept in gauge_data and written to its file."""
+        ix, iy = state.grid.gauges[i][0], state.grid.gauges[i][1]
+        aux = state._aux[:, ix, iy] if state.num_aux > 0 else None
+        p = self.compute_gauge_values(q, aux)
+        if state.keep_gauges:
+            gauge_data = state.gauge_data
+            if len(gauge_data) == len(state.grid.gauges):
+                gauge_data[i] = np.vstack((gauge_data[i], np.append(t, p)))
+            else:
+                gauge_data.append(np.append(t, p))
+        try:
+            state.grid.gauge_files[i].write(str(t) + ' ' + ' '.join(str(j) for j in p) + '\n')
+        except Exception:
+            raise Exception("Gauge files are not set up correctly. You should call the method "
+                            "`setup_gauge_files` of the Grid class object before any call for "
+                            "`write_gauge_values` from the Solver class.")

@@ -333,3 +333,67 @@ def test_session_step2_host_buffers(orc):
         assert np.array_equal(qnew[:, 2:-2, 2:-2], ref[:, 2:-2, 2:-2])
     finally:
         lib.claw2_session_destroy(s)
+
+
+def _gauged_vc_run(outdir, host_loop, orc=None):
+    """apps/acoustics_2d_variable at 80x80 with four gauges (the psystem app's
+    way of adding them, apps/psystem_2d/psystem.py:224-227) and a
+    compute_gauge_values of q and aux, run to t = 0.4 through Controller.run."""
+    p, q, aux, run = K.acoustics_variable_setup(mx=80, my=80)
+    x = pc.Dimension('x', -1.0, 1.0, p.mx)
+    y = pc.Dimension('y', -1.0, 1.0, p.my)
+    domain = pc.Domain([x, y])
+    state = pc.State(domain, 3, 2)
+    state.q[...] = q
+    state.aux[...] = aux
+    state.keep_gauges = True
+    state.grid.add_gauges([[-0.5, 0.0], [0.25, 0.3], [0.9, -0.9], [-0.95, 0.95]])
+    solver = pc.ClawSolver2D(pc.riemann.rp2_vc_acoustics)
+    solver.dimensional_split = False
+    solver.transverse_waves = 1
+    solver.limiters = pc.limiters.tvd.MC
+    solver.bc_lower = [pc.BC.wall, pc.BC.wall]
+    solver.bc_upper = [pc.BC.extrap, pc.BC.extrap]
+    solver.aux_bc_lower = [pc.BC.wall, pc.BC.wall]
+    solver.aux_bc_upper = [pc.BC.extrap, pc.BC.extrap]
+    solver.dt_initial = run['dt_initial']
+    solver.compute_gauge_values = lambda qg, ag: [qg[0] * ag[0], qg[1] + qg[2]]
+    if host_loop:
+        solver.before_step = lambda s, st: None           # forces the host-driven loop
+    claw = pc.Controller()
+    claw.solution = pc.Solution(state, domain)
+    claw.solver = solver
+    claw.outdir = outdir
+    claw.output_format = None
+    claw.tfinal = 0.4
+    claw.num_output_times = 4
+    claw.run()
+    return claw, solver, state, (p, q, aux, run)
+
+
+def test_gauges_recorded_on_the_device(orc, tmp_path):
+    """Gauges keep the time loop on the device (samples recorded after every
+    accepted step, drained after each batch of steps) and give exactly what
+    write_gauge_values gives on the host-driven loop, in memory and in the
+    gauge files; the last samples equal the oracle's final state."""
+    claw_d, solver_d, st_d, (p, q, aux, run) = _gauged_vc_run(str(tmp_path / "dev"), host_loop=False)
+    assert solver_d._device_loop_ok(claw_d.solution)
+    claw_h, solver_h, st_h, _ = _gauged_vc_run(str(tmp_path / "host"), host_loop=True)
+    assert not solver_h._device_loop_ok(claw_h.solution)
+    assert len(st_d.gauge_data) == 4
+    nsteps = solver_d.status['numsteps']
+    for gd, gh in zip(st_d.gauge_data, st_h.gauge_data):
+        assert gd.shape == gh.shape and gd.shape[0] >= 2
+        assert np.array_equal(gd, gh)
+    for name in st_d.grid.gauge_file_names:
+        with open(os.path.join(str(tmp_path / "dev"), "_gauges", name)) as f:
+            text_d = f.read()
+        with open(os.path.join(str(tmp_path / "host"), "_gauges", name)) as f:
+            text_h = f.read()
+        assert text_d == text_h and len(text_d.splitlines()) >= nsteps
+    ref = orc.Run(p, q, aux, **run)
+    frames = ref.run(0.4, num_output_times=4)
+    for i, (ix, iy) in enumerate(st_d.grid.gauges):
+        qg = frames[-1][:, ix, iy]
+        assert st_d.gauge_data[i][-1][0] == ref.t
+        assert list(st_d.gauge_data[i][-1][1:]) == [qg[0] * aux[0, ix, iy], qg[1] + qg[2]]
