@@ -93,16 +93,24 @@ lean_step_kernel(StepArgs a, const __grid_constant__ CUtensorMap tm0, const __gr
 }
 
 // Instance of tile t: the last one with tile_begin <= t (binary search).
-__device__ __forceinline__ int batch_instance_of(const claw2_batch_instance* __restrict__ inst, int ninst, int t)
+// With tb (the instances' tile_begin copied into shared memory by the
+// kernel) the search reads shared memory instead of walking the descriptors
+// in global memory, a chain of dependent L2 loads per tile.
+__device__ __forceinline__ int batch_instance_of(const claw2_batch_instance* __restrict__ inst, int ninst, int t,
+                                                 const int* tb = nullptr)
 {
     int lo = 0, hi = ninst - 1;
     while (lo < hi) {
         const int mid = (lo + hi + 1) >> 1;
-        if (__ldg(&inst[mid].tile_begin) <= t) lo = mid;
+        if ((tb ? tb[mid] : __ldg(&inst[mid].tile_begin)) <= t) lo = mid;
         else hi = mid - 1;
     }
     return lo;
 }
+
+// batches of at most this many instances keep their tile_begin table in
+// shared memory (4 bytes each)
+constexpr int kBatchTableMax = 4096;
 
 // Ask L2 for the input halo of tile t (rows j0-2..j0+TY+1 and columns
 // i0-2..i0+TX+1, clipped to the ghosted arrays, of the current state and of
@@ -112,9 +120,10 @@ __device__ __forceinline__ int batch_instance_of(const claw2_batch_instance* __r
 // addresses stay inside the instance's arrays; results do not depend on it.
 // Returns tile t's instance.
 template <int MEQN, int MAUX, int TX, int TY, int NT>
-__device__ __forceinline__ int batch_prefetch_tile(const claw2_batch_instance* __restrict__ inst, int ninst, int t)
+__device__ __forceinline__ int batch_prefetch_tile(const claw2_batch_instance* __restrict__ inst, int ninst, int t,
+                                                   const int* tb)
 {
-    const int k = batch_instance_of(inst, ninst, t);
+    const int k = batch_instance_of(inst, ninst, t, tb);
     const claw2_batch_instance& I = inst[k];
     const claw2_control* c = I.ctrl;
     if (c->done) return k;
@@ -140,18 +149,27 @@ __device__ __forceinline__ int batch_prefetch_tile(const claw2_batch_instance* _
 // Batched step: a persistent grid walks the concatenated tile list of all
 // instances; each tile (T x T cells) is one tile-body call with that
 // instance's buffers, with an L2 prefetch of the CTA's next tile issued first.
+// body_doubles: the tile body's shared memory; with `table` set the
+// instances' tile_begin table follows it.
 template <class RP, int NT, int MINB, bool LIGHT, int T>
 __global__ void __launch_bounds__(NT, MINB)
-batch_kernel(const claw2_batch_instance* __restrict__ inst, int ninst, int ntiles, StepArgs common)
+batch_kernel(const claw2_batch_instance* __restrict__ inst, int ninst, int ntiles, StepArgs common, int body_doubles,
+             int table)
 {
     static_assert(LIGHT || T == 29, "the generic body runs 29x29 tiles in the batch");
     extern __shared__ double smem_dyn[];
     DevCtx ctx{smem_dyn};
+    int* tb = nullptr;
+    if (table) {
+        tb = reinterpret_cast<int*>(smem_dyn + body_doubles);
+        for (int i = threadIdx.x; i < ninst; i += NT) tb[i] = __ldg(&inst[i].tile_begin);
+        __syncthreads();
+    }
     int next = -1;                                  // instance of the next tile, found by its prefetch
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-        const int lo = next >= 0 ? next : batch_instance_of(inst, ninst, t);
+        const int lo = next >= 0 ? next : batch_instance_of(inst, ninst, t, tb);
         next = t + (int)gridDim.x < ntiles
-                   ? batch_prefetch_tile<RP::MEQN, RP::MAUX, T, T, NT>(inst, ninst, t + (int)gridDim.x)
+                   ? batch_prefetch_tile<RP::MEQN, RP::MAUX, T, T, NT>(inst, ninst, t + (int)gridDim.x, tb)
                    : -1;
         const claw2_batch_instance& I = inst[lo];
         StepArgs a = common;
@@ -869,14 +887,24 @@ int batch_launch_t(const StepArgs& common, const claw2_batch_instance* inst, int
                    cudaStream_t st)
 {
     constexpr int SMB = LIGHT ? LightSmem<T, T, NT>::bytes : TileSmem<RP, 29, 29, NT, false>::bytes;
+    constexpr int kSmemLimit = 227 * 1024;        // dynamic shared memory a CTA can opt in to
+    constexpr int SMMAX = SMB + 4 * kBatchTableMax < kSmemLimit ? SMB + 4 * kBatchTableMax : SMB;
     auto kern = batch_kernel<RP, NT, MINB, LIGHT, T>;
     static std::atomic<uint64_t> optin{0};
-    static std::atomic<int> grids[kDevAttrSlots];
-    const int grid = persistent_grid(optin, grids, kern, NT, SMB);
-    if (grid < 1) return CLAW2_ERR_CUDA;
+    if (smem_optin(optin, kern, SMMAX) != cudaSuccess) return CLAW2_ERR_CUDA;
+    // the persistent grid: SMs x the CTAs that fit with this launch's table
+    const int tbytes = (4 * ninst + 15) / 16 * 16;
+    const int table = ninst <= kBatchTableMax && SMB + tbytes <= SMMAX;
+    const int smem = SMB + (table ? tbytes : 0);
+    int dev = 0, nsm = 0, occ = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, NT, smem) != cudaSuccess || occ < 1)
+        return CLAW2_ERR_CUDA;
+    const int grid = nsm * occ;
     const int g = ntiles < grid ? ntiles : grid;
     for (int n = 0; n < nsteps; n++) {
-        kern<<<g, NT, SMB, st>>>(inst, ninst, ntiles, common);
+        kern<<<g, NT, smem, st>>>(inst, ninst, ntiles, common, SMB / 8, table);
         if (cudaGetLastError() != cudaSuccess) return CLAW2_ERR_CUDA;
     }
     return CLAW2_OK;

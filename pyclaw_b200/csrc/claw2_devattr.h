@@ -32,28 +32,4 @@ inline cudaError_t smem_optin(std::atomic<uint64_t>& mask, F kern, int bytes)
     return cudaSuccess;
 }
 
-// Persistent-grid size (SM count x resident CTAs) of `kern` on the current
-// device, after its shared-memory opt-in; `cache` (one per kernel) holds it
-// per device ordinal < 64.  Returns 0 on a CUDA error.
-template <class F>
-inline int persistent_grid(std::atomic<uint64_t>& mask, std::atomic<int> (&cache)[kDevAttrSlots], F kern, int threads,
-                           int bytes)
-{
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess) return 0;
-    const bool slot = dev >= 0 && dev < kDevAttrSlots;
-    if (slot) {
-        const int g = cache[dev].load(std::memory_order_acquire);
-        if (g > 0) return g;
-    }
-    if (smem_optin(mask, kern, bytes) != cudaSuccess) return 0;
-    int nsm = 0, occ = 0;
-    if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, threads, bytes) != cudaSuccess || occ < 1)
-        return 0;
-    const int g = nsm * occ;
-    if (slot) cache[dev].store(g, std::memory_order_release);
-    return g;
-}
-
 }  // namespace claw2

@@ -51,6 +51,17 @@ template <class RP, int TX, int TY, int NT> struct LeanSmem {
     static_assert((BOX * 8) % 1024 == 0, "each box starts on a 1024-byte boundary");
 };
 
+// f(IntC<0>{}), ..., f(IntC<N-1>{}): a loop whose index is a compile-time constant
+template <int N> struct IntC { static constexpr int value = N; };
+template <int N, int I = 0, class F>
+__device__ __forceinline__ void static_for(F&& f)
+{
+    if constexpr (I < N) {
+        f(IntC<I>{});
+        static_for<N, I + 1>(f);
+    }
+}
+
 // The staged input of halo row r, column c, field m: H holds q(m, i0-2+c, j0-2+r).
 template <int MEQN, int TR>
 __device__ __forceinline__ int lean_hidx(int m, int r, int c)
@@ -82,13 +93,12 @@ CLAW2_HD void lean_chunk(const StepArgs& a, Ctx& ctx, const double* H, double* Q
     const bool lim = ifok && slot >= 1 && slot <= NSLOT - 2 && k >= 0 && k <= len;
 
     // ---------------- normal solve ----------------
-    double wave[MW][MEQN], s[MW], amdq[MEQN], apdq[MEQN], roe[NROE];
+    // the waves are kept as their strengths: wave p is alpha[p] times rpn2c's
+    // eigenvector of the Roe averages, rebuilt with the same operations where
+    // it is needed (RP::wave_of), and s[p] is RP::speed<p>(roe)
+    double alpha[MW], amdq[MEQN], apdq[MEQN], roe[NROE];
 #pragma unroll
-    for (int p = 0; p < MW; p++) {
-        s[p] = 0.0;
-#pragma unroll
-        for (int m = 0; m < MEQN; m++) wave[p][m] = 0.0;
-    }
+    for (int p = 0; p < MW; p++) alpha[p] = 0.0;
 #pragma unroll
     for (int m = 0; m < MEQN; m++) { amdq[m] = 0.0; apdq[m] = 0.0; }
 #pragma unroll
@@ -106,51 +116,59 @@ CLAW2_HD void lean_chunk(const StepArgs& a, Ctx& ctx, const double* H, double* Q
             double qR[MEQN];
 #pragma unroll
             for (int m = 0; m < MEQN; m++) qR[m] = hq(m, k, line);
-            RP::template rpn2c<IXY>(qL, qR, L, R, a.prm, wave, s, amdq, apdq, roe);
+            RP::template rpn2a<IXY>(qL, qR, L, R, a.prm, alpha, amdq, apdq, roe);
         }
     }
 
     // ---------------- CFL, limiter, second-order corrections ----------------
     if (lim) {
-#pragma unroll
-        for (int p = 0; p < MW; p++) {
-            const double c1 = dtn * s[p], c2 = -dtn * s[p];
+        static_for<MW>([&](auto P) {
+            const double sp = RP::template speed<decltype(P)::value>(roe);
+            const double c1 = dtn * sp, c2 = -dtn * sp;
             cflm = cflm > c1 ? cflm : c1;
             cflm = cflm > c2 ? cflm : c2;
-        }
+        });
     }
     double cqxx[MEQN], fadd[MEQN];
 #pragma unroll
     for (int m = 0; m < MEQN; m++) { cqxx[m] = 0.0; fadd[m] = 0.0; }
     if (a.order == 2) {                       // uniform: every lane takes part in the shuffles
         const double dtdxave = 0.5 * (dtn + dtn);
+        // the right neighbour's strengths and the Roe averages its waves use
+        double alr[MW], roer[NROE];
 #pragma unroll
-        for (int p = 0; p < MW; p++) {
+        for (int p = 0; p < MW; p++) alr[p] = ctx.shfl_down(alpha[p]);
+#pragma unroll
+        for (int r = 0; r < NROE; r++) roer[r] = r < RP::NROE_WAVE ? ctx.shfl_down(roe[r]) : 0.0;
+        static_for<MW>([&](auto P) {
+            constexpr int p = decltype(P)::value;
+            double wv[MEQN], wn[MEQN];
+            RP::template wave_of<IXY, p>(alpha[p], roe, wv);
+            RP::template wave_of<IXY, p>(alr[p], roer, wn);
+            // dotr = wave(k).wave(k+1); dotl of lane k is dotr of lane k-1
             double dotr = 0.0;
 #pragma unroll
-            for (int m = 0; m < MEQN; m++) dotr = dotr + wave[p][m] * ctx.shfl_down(wave[p][m]);
+            for (int m = 0; m < MEQN; m++) dotr = dotr + wv[m] * wn[m];
             const double dotl = ctx.shfl_up(dotr);
+            const double sp = RP::template speed<p>(roe);
             if (lim) {
-                double wv[MEQN];
-#pragma unroll
-                for (int m = 0; m < MEQN; m++) wv[m] = wave[p][m];
                 const int meth = a.mthlim[p];
                 if (a.limit_any && meth != 0) {
                     double wnorm2 = 0.0;
 #pragma unroll
                     for (int m = 0; m < MEQN; m++) wnorm2 = wnorm2 + wv[m] * wv[m];
                     if (wnorm2 != 0.0) {
-                        const double phi = philim(wnorm2, s[p] > 0.0 ? dotl : dotr, meth);
+                        const double phi = philim(wnorm2, sp > 0.0 ? dotl : dotr, meth);
 #pragma unroll
                         for (int m = 0; m < MEQN; m++) wv[m] = phi * wv[m];
                     }
                 }
-                const double as = fabs(s[p]);
+                const double as = fabs(sp);
                 const double f = as * (1.0 - as * dtdxave);
 #pragma unroll
                 for (int m = 0; m < MEQN; m++) cqxx[m] = (p == 0) ? f * wv[m] : cqxx[m] + f * wv[m];
             }
-        }
+        });
 #pragma unroll
         for (int m = 0; m < MEQN; m++) fadd[m] = 0.5 * cqxx[m];
     }
@@ -168,8 +186,13 @@ CLAW2_HD void lean_chunk(const StepArgs& a, Ctx& ctx, const double* H, double* Q
             Pf[m] = cor ? apdq[m] - cqxx[m] : apdq[m];
         }
         const double noaux[1] = {0.0};
-        RP::template rpt2<IXY>(1, A, roe, noaux, noaux, noaux, a.prm, bmL, bpL);
-        RP::template rpt2<IXY>(2, Pf, roe, noaux, noaux, noaux, a.prm, bmR, bpR);
+        // a zero fluctuation splits into zeros (up to the sign of zero), so
+        // its transverse solve is skipped
+        bool nzA = false, nzP = false;
+#pragma unroll
+        for (int m = 0; m < MEQN; m++) { nzA = nzA || A[m] != 0.0; nzP = nzP || Pf[m] != 0.0; }
+        if (nzA) RP::template rpt2<IXY>(1, A, roe, noaux, noaux, noaux, a.prm, bmL, bpL);
+        if (nzP) RP::template rpt2<IXY>(2, Pf, roe, noaux, noaux, noaux, a.prm, bmR, bpR);
     }
 
     // ---------------- the slice's contributions to cell k ----------------
@@ -178,10 +201,12 @@ CLAW2_HD void lean_chunk(const StepArgs& a, Ctx& ctx, const double* H, double* Q
     double y0[MEQN], y1[MEQN], y2[MEQN], y3[MEQN];
 #pragma unroll
     for (int m = 0; m < MEQN; m++) {
-        y0[m] = ctx.shfl_down(lim ? dtn * amdq[m] : 0.0);
-        y1[m] = ctx.shfl_down(lim ? fadd[m] : 0.0);
-        y2[m] = ctx.shfl_down(lim ? hl * bmL[m] : 0.0);
-        y3[m] = ctx.shfl_down(lim ? hl * bpL[m] : 0.0);
+        // a cell-owning lane (cellok) takes these from lane k+1, which is
+        // always a limited interface (lim), so no lane needs them zeroed
+        y0[m] = ctx.shfl_down(dtn * amdq[m]);
+        y1[m] = ctx.shfl_down(fadd[m]);
+        y2[m] = ctx.shfl_down(hl * bmL[m]);
+        y3[m] = ctx.shfl_down(hl * bpL[m]);
     }
     const bool cellok = lim && slot <= NCELL && k < len;
     const bool trans = a.trans > 0;

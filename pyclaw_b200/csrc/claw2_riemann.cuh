@@ -105,6 +105,25 @@ template <bool TRACER> struct RpEuler {
         const double d1 = qR[mu] - qL[mu];
         const double d2 = qR[mv] - qL[mv];
         const double d3 = qR[3] - qL[3];
+        bool same = d0 == 0.0 && d1 == 0.0 && d2 == 0.0 && d3 == 0.0;
+        if constexpr (TRACER) same = same && qR[4] - qL[4] == 0.0;
+        if (same) {
+            // Equal states: every strength is zero, so every wave and, through
+            // the entropy fix (whose s1 equals s0 here, so no transonic split)
+            // and apdq = sum s*wave - amdq, both fluctuations are zero; only the
+            // sign of a zero can differ from computing them.  The speeds still
+            // count in the CFL number.
+#pragma unroll
+            for (int p = 0; p < MW; p++) {
+#pragma unroll
+                for (int m = 0; m < MEQN; m++) wave[p][m] = 0.0;
+            }
+            s[0] = u - a; s[1] = u; s[2] = u; s[3] = u + a;
+            if constexpr (TRACER) s[4] = u;
+#pragma unroll
+            for (int m = 0; m < MEQN; m++) { amdq[m] = 0.0; apdq[m] = 0.0; }
+            return;
+        }
         const double a3 = g1a2 * (euv * d0 + u * d1 + v * d2 - d3);
         const double a2 = d2 - v * d0;
         const double a4 = (d1 + (a - u) * d0 - a * a3) / (2.0 * a);
@@ -200,6 +219,47 @@ template <bool TRACER> struct RpEuler {
             apdq[3] = dfe - amdq[3];
             if constexpr (TRACER) apdq[4] = s[4] * wave[4][4] - amdq[4];
         }
+    }
+
+    // The lean tile body keeps an interface's waves as their strengths alpha[p]
+    // and rebuilds wave p from alpha[p] and the Roe averages with rpn2c's own
+    // expressions (same operands, same operations: the same bits), which holds
+    // 4-5 doubles per interface instead of 16-25 through the limiter.
+    static constexpr int NROE_WAVE = 5;          // u, v, a, enth, u2v2 build the waves
+    template <int IXY, int P>
+    static CLAW2_DEV void wave_of(double al, const double (&roe)[NROE], double (&w)[MEQN])
+    {
+        constexpr int mu = Dir<IXY>::MU, mv = Dir<IXY>::MV;
+        const double u = roe[0], v = roe[1], a = roe[2], enth = roe[3], u2v2 = roe[4];
+        if constexpr (P == 0) { w[0] = al; w[mu] = al * (u - a); w[mv] = al * v; w[3] = al * (enth - u * a); }
+        else if constexpr (P == 1) { w[0] = 0.0; w[mu] = 0.0; w[mv] = al; w[3] = al * v; }
+        else if constexpr (P == 2) { w[0] = al; w[mu] = al * u; w[mv] = al * v; w[3] = al * 0.5 * u2v2; }
+        else if constexpr (P == 3) { w[0] = al; w[mu] = al * (u + a); w[mv] = al * v; w[3] = al * (enth + u * a); }
+        else { w[0] = 0.0; w[1] = 0.0; w[2] = 0.0; w[3] = 0.0; }
+        if constexpr (TRACER) w[4] = P == 4 ? al : 0.0;
+    }
+    // speed of wave P (rpn2c's s[P])
+    template <int P>
+    static CLAW2_DEV double speed(const double (&roe)[NROE])
+    {
+        if constexpr (P == 0) return roe[0] - roe[2];
+        else if constexpr (P == 3) return roe[0] + roe[2];
+        else return roe[0];
+    }
+    // rpn2c returning the wave strengths instead of the waves and speeds
+    template <int IXY>
+    static CLAW2_DEV void rpn2a(const double (&qL)[MEQN], const double (&qR)[MEQN], const Cell& L, const Cell& R,
+                                const double* prm, double (&alpha)[MW], double (&amdq)[MEQN], double (&apdq)[MEQN],
+                                double (&roe)[NROE])
+    {
+        constexpr int mv = Dir<IXY>::MV;
+        double wave[MW][MEQN], s[MW];
+        rpn2c<IXY>(qL, qR, L, R, prm, wave, s, amdq, apdq, roe);
+        alpha[0] = wave[0][0];
+        alpha[1] = wave[1][mv];
+        alpha[2] = wave[2][0];
+        alpha[3] = wave[3][0];
+        if constexpr (TRACER) alpha[4] = wave[4][4];
     }
 
     // rpt2_euler_5wave.f:47-95.  The split uses this interface's Roe averages.
@@ -379,10 +439,23 @@ struct RpShallow {
         const double delta1 = hr - hl;
         const double delta2 = qR[mu] - qL[mu];
         const double delta3 = qR[mv] - qL[mv];
+        roe[0] = ubar; roe[1] = vbar; roe[2] = cbar;
+        if (delta1 == 0.0 && delta2 == 0.0 && delta3 == 0.0) {
+            // equal states: zero waves and fluctuations (see RpEuler::rpn2c);
+            // the speeds still count in the CFL number
+#pragma unroll
+            for (int p = 0; p < MW; p++) {
+#pragma unroll
+                for (int m = 0; m < MEQN; m++) wave[p][m] = 0.0;
+            }
+            s[0] = ubar - cbar; s[1] = ubar; s[2] = ubar + cbar;
+#pragma unroll
+            for (int m = 0; m < MEQN; m++) { amdq[m] = 0.0; apdq[m] = 0.0; }
+            return;
+        }
         const double a1 = ((ubar + cbar) * delta1 - delta2) / (2.0 * cbar);
         const double a2 = delta3 - vbar * delta1;
         const double a3 = (delta2 - (ubar - cbar) * delta1) / (2.0 * cbar);
-        roe[0] = ubar; roe[1] = vbar; roe[2] = cbar;
         wave[0][0] = a1; wave[0][mu] = a1 * (ubar - cbar); wave[0][mv] = a1 * vbar; s[0] = ubar - cbar;
         wave[1][0] = 0.0; wave[1][mu] = 0.0; wave[1][mv] = a2; s[1] = ubar;
         wave[2][0] = a3; wave[2][mu] = a3 * (ubar + cbar); wave[2][mv] = a3 * vbar; s[2] = ubar + cbar;
@@ -426,6 +499,37 @@ struct RpShallow {
         apdq[0] = df0 - amdq[0];
         apdq[mu] = dfu - amdq[mu];
         apdq[mv] = dfv - amdq[mv];
+    }
+
+    // waves as strengths times rpn2c's eigenvectors (see RpEuler::wave_of)
+    static constexpr int NROE_WAVE = 3;          // ubar, vbar, cbar
+    template <int IXY, int P>
+    static CLAW2_DEV void wave_of(double al, const double (&roe)[NROE], double (&w)[MEQN])
+    {
+        constexpr int mu = Dir<IXY>::MU, mv = Dir<IXY>::MV;
+        const double ubar = roe[0], vbar = roe[1], cbar = roe[2];
+        if constexpr (P == 0) { w[0] = al; w[mu] = al * (ubar - cbar); w[mv] = al * vbar; }
+        else if constexpr (P == 1) { w[0] = 0.0; w[mu] = 0.0; w[mv] = al; }
+        else { w[0] = al; w[mu] = al * (ubar + cbar); w[mv] = al * vbar; }
+    }
+    template <int P>
+    static CLAW2_DEV double speed(const double (&roe)[NROE])
+    {
+        if constexpr (P == 0) return roe[0] - roe[2];
+        else if constexpr (P == 2) return roe[0] + roe[2];
+        else return roe[0];
+    }
+    template <int IXY>
+    static CLAW2_DEV void rpn2a(const double (&qL)[MEQN], const double (&qR)[MEQN], const Cell& L, const Cell& R,
+                                const double* prm, double (&alpha)[MW], double (&amdq)[MEQN], double (&apdq)[MEQN],
+                                double (&roe)[NROE])
+    {
+        constexpr int mv = Dir<IXY>::MV;
+        double wave[MW][MEQN], s[MW];
+        rpn2c<IXY>(qL, qR, L, R, prm, wave, s, amdq, apdq, roe);
+        alpha[0] = wave[0][0];
+        alpha[1] = wave[1][mv];
+        alpha[2] = wave[2][0];
     }
 
     template <int IXY>
