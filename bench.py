@@ -1035,7 +1035,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--headline-only", action="store_true",
                     help="only the shock-bubble line, without the batched / adjoint / shallow / acoustics parts")
-    ap.add_argument("--develop", type=int, default=1000,
+    ap.add_argument("--develop", type=int, default=1500,
                     help="untimed steps of set-up before the warm-up (shock bubble)")
     ap.add_argument("--split", action="store_true",
                     help="shock bubble with dimensional splitting (the reference's default mode)")

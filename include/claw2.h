@@ -69,7 +69,9 @@ enum claw2_rp {
     CLAW2_RP_VC_ACOUSTICS = 2,    /* rp2_vc_acoustics: q=(p,u,v), aux=(rho,c)         */
     CLAW2_RP_EULER_4WAVE = 3,     /* rp2_euler_4wave: q=(rho,rhou,rhov,E); gamma,gamma1 */
     CLAW2_RP_EULER_5WAVE = 4,     /* rp2_euler_5wave: + tracer; gamma,gamma1          */
-    CLAW2_RP_SHALLOW_ROE = 5      /* rp2_shallow_roe_with_efix: q=(h,hu,hv); grav     */
+    CLAW2_RP_SHALLOW_ROE = 5,     /* rp2_shallow_roe_with_efix: q=(h,hu,hv); grav     */
+    CLAW2_RP_PSYSTEM = 6          /* rp2_psystem (f-waves): q=(eps,rho u,rho v),
+                                     aux=(rho, K, linearity 1|2, eps for rpt2)      */
 };
 
 /* ---- boundary conditions (pyclaw.BC, src/pyclaw/solver.py:12-18) ------- */
@@ -237,10 +239,19 @@ enum claw2_source {
 typedef struct claw2_hooks {
     int32_t source;        /* claw2_source                                  */
     int32_t source_aux;    /* aux component holding the radial coordinate   */
-    int32_t reserved_[2];
+    int32_t aux_from_q;    /* 0, or k: before every step aux component k     */
+    int32_t aux_q;         /*   (1-based) is set to q component aux_q        */
+                           /*   (1-based) of the current state, ghost cells  */
+                           /*   included (aux is written: it must be device  */
+                           /*   memory the library may change)               */
 } claw2_hooks;
 
-/* claw2_advance with the source term of `hooks` applied to each step.
+/* claw2_advance with the hooks applied to each step: the source term, and
+ * the before-step copy of a state component into an aux component that the
+ * Riemann solver reads (apps/psystem_2d/psystem.py:86-90 sets aux(4) = q(1)
+ * before every step for its transverse solver).  The copy takes the ghost
+ * cells of q too, so the aux boundary conditions of that component must be
+ * those of q (checked: CLAW2_ERR_UNSUPPORTED otherwise).
  * CLAW2_ERR_UNSUPPORTED for a source the Riemann solver cannot take
  * (CLAW2_SRC_EULER_RADIAL needs the Euler solvers and aux). */
 CLAW2_EXPORT int claw2_advance_hooked(const claw2_problem* p, double* q0, double* q1, const double* aux,

@@ -19,6 +19,8 @@
  *   philim          src/pyclaw/classic/philim.f90:18-55
  *   rpn2_euler      development/rp_approaches/rpn2_euler_5wave.f:63-298
  *   rpt2_euler      development/rp_approaches/rpt2_euler_5wave.f:39-95
+ *   rpn2/rpt2_psystem  the f-wave p-system of apps/psystem_2d (restated from
+ *                   its equations; pinned by apps/psystem_2d/verify_gauge*.txt)
  *   orc_fill_bc     src/pyclaw/solver.py:299-434 (q) and :438-576 (aux)
  *   orc_evolve      src/pyclaw/solver.py:582-699 with classic/solver.py:100-151
  * The acoustics, variable-coefficient acoustics and shallow-water Riemann
@@ -415,6 +417,79 @@ static void rpt2_shallow(int ixy, int mx, int meqn, int mbc, const double* asdq,
     }
 }
 
+/* Two-dimensional p-system (nonlinear elasticity in layered media,
+ * apps/psystem_2d/psystem.py): eps_t - u_x - v_y = 0, (rho u)_t - sigma_x = 0,
+ * (rho v)_t - sigma_y = 0 with u = (rho u)/rho, aux = (rho, K, linearity, eps),
+ * sigma = K eps (linearity 1) or exp(K eps) - 1 (linearity 2).  f-wave solver:
+ * the flux jump f(q_i, x_i) - f(q_{i-1}, x_{i-1}), f = (-u, -sigma, 0) along the
+ * normal, split on the eigenvectors (1, Z_{i-1}) with speed -c_{i-1} and
+ * (1, -Z_i) with speed c_i, c = sqrt(sigma_eps / rho), Z = rho c (LeVeque 2002,
+ * sec. 15.5 on f-waves; the same pairing of left and right materials as the
+ * variable-coefficient acoustics solver). */
+static void psys_cell(const double* aux, double eps, double* sigma, double* c, double* z)
+{
+    const double rho = aux[0], K = aux[1];
+    double se;
+    if (aux[2] == 1.0) { *sigma = K * eps; se = K; }
+    else { const double e = exp(K * eps); *sigma = e - 1.0; se = K * e; }
+    *c = sqrt(se / rho);
+    *z = rho * *c;
+}
+
+static void rpn2_psystem(int ixy, int mx, int meqn, int mwaves, int mbc, int maux,
+                         const double* ql, const double* qr, const double* auxl,
+                         const double* auxr, double* wave, double* s,
+                         double* amdq, double* apdq)
+{
+    int mu, mv, i, m;
+    if (ixy == 1) { mu = 2; mv = 3; } else { mu = 3; mv = 2; }
+    for (i = 2 - mbc; i <= mx + mbc; i++) {
+        double sgl, cl, zl, sgr, cr, zr;
+        psys_cell(&AUXS(auxr, 1, i - 1), Q1D(qr, 1, i - 1), &sgl, &cl, &zl);
+        psys_cell(&AUXS(auxl, 1, i), Q1D(ql, 1, i), &sgr, &cr, &zr);
+        const double ul = Q1D(qr, mu, i - 1) / AUXS(auxr, 1, i - 1);
+        const double ur = Q1D(ql, mu, i) / AUXS(auxl, 1, i);
+        const double df1 = (-ur) - (-ul);
+        const double df2 = (-sgr) - (-sgl);
+        const double b1 = (zr * df1 + df2) / (zl + zr);
+        const double b2 = (zl * df1 - df2) / (zl + zr);
+        WAVE(1, 1, i) = b1; WAVE(mu, 1, i) = b1 * zl; WAVE(mv, 1, i) = 0.0;
+        SPD(1, i) = -cl;
+        WAVE(1, 2, i) = b2; WAVE(mu, 2, i) = -b2 * zr; WAVE(mv, 2, i) = 0.0;
+        SPD(2, i) = cr;
+        for (m = 1; m <= meqn; m++) {
+            Q1D(amdq, m, i) = WAVE(m, 1, i);
+            Q1D(apdq, m, i) = WAVE(m, 2, i);
+        }
+    }
+}
+
+/* Transverse p-system: asdq sits in cell i1 = i-2+ilr; it is split on the
+ * eigenvectors of the cells across the slice, (1, Z_b) going down with speed
+ * -c_b in the cell below and (1, -Z_a) going up with speed c_a in the cell
+ * above, with eps of those cells from aux(4) (set from q before each step by
+ * the application, apps/psystem_2d/psystem.py:87-90).  This split reproduces
+ * the reference's gauge files (apps/psystem_2d/verify_gauge*.txt) to their
+ * printed digits; pairing either part with the cell's own eigenvector does
+ * not (3e-5 after one step). */
+static void rpt2_psystem(int ixy, int mx, int meqn, int mbc, int maux, int ilr,
+                         const double* aux1, const double* aux2, const double* aux3,
+                         const double* asdq, double* bmasdq, double* bpasdq)
+{
+    int mu, mv, i;
+    if (ixy == 1) { mu = 2; mv = 3; } else { mu = 3; mv = 2; }
+    for (i = 2 - mbc; i <= mx + mbc; i++) {
+        int i1 = i - 2 + ilr;
+        double sgb, cb, zb, sga, ca, za;
+        psys_cell(&AUXS(aux1, 1, i1), AUXS(aux1, 4, i1), &sgb, &cb, &zb);
+        psys_cell(&AUXS(aux3, 1, i1), AUXS(aux3, 4, i1), &sga, &ca, &za);
+        const double gb = (za * Q1D(asdq, 1, i) + Q1D(asdq, mv, i)) / (zb + za);
+        const double ga = (zb * Q1D(asdq, 1, i) - Q1D(asdq, mv, i)) / (zb + za);
+        Q1D(bmasdq, 1, i) = -cb * gb; Q1D(bmasdq, mu, i) = 0.0; Q1D(bmasdq, mv, i) = -cb * gb * zb;
+        Q1D(bpasdq, 1, i) = ca * ga; Q1D(bpasdq, mu, i) = 0.0; Q1D(bpasdq, mv, i) = -ca * ga * za;
+    }
+}
+
 static void call_rpn2(int ixy, int mx, int meqn, int mwaves, int mbc, int maux,
                       const double* q1d, const double* aux2, double* wave, double* s,
                       double* amdq, double* apdq, orc_ctx* ctx)
@@ -425,6 +500,7 @@ static void call_rpn2(int ixy, int mx, int meqn, int mwaves, int mbc, int maux,
     case CLAW2_RP_EULER_4WAVE:  rpn2_euler(ixy, mx, meqn, mwaves, mbc, q1d, q1d, wave, s, amdq, apdq, ctx, 0); break;
     case CLAW2_RP_EULER_5WAVE:  rpn2_euler(ixy, mx, meqn, mwaves, mbc, q1d, q1d, wave, s, amdq, apdq, ctx, 1); break;
     case CLAW2_RP_SHALLOW_ROE:  rpn2_shallow(ixy, mx, meqn, mwaves, mbc, q1d, q1d, wave, s, amdq, apdq, ctx); break;
+    case CLAW2_RP_PSYSTEM:      rpn2_psystem(ixy, mx, meqn, mwaves, mbc, maux, q1d, q1d, aux2, aux2, wave, s, amdq, apdq); break;
     }
 }
 
@@ -438,6 +514,7 @@ static void call_rpt2(int ixy, int mx, int meqn, int mbc, int maux, int ilr,
     case CLAW2_RP_EULER_4WAVE:  rpt2_euler(ixy, mx, meqn, mbc, asdq, bmasdq, bpasdq, ctx, 0); break;
     case CLAW2_RP_EULER_5WAVE:  rpt2_euler(ixy, mx, meqn, mbc, asdq, bmasdq, bpasdq, ctx, 1); break;
     case CLAW2_RP_SHALLOW_ROE:  rpt2_shallow(ixy, mx, meqn, mbc, asdq, bmasdq, bpasdq, ctx); break;
+    case CLAW2_RP_PSYSTEM:      rpt2_psystem(ixy, mx, meqn, mbc, maux, ilr, aux1, aux2, aux3, asdq, bmasdq, bpasdq); break;
     }
 }
 
@@ -615,6 +692,7 @@ static int check_problem(const claw2_problem* p)
     case CLAW2_RP_EULER_4WAVE: if (p->num_eqn != 4 || p->num_waves != 4) return CLAW2_ERR_INVALID; break;
     case CLAW2_RP_EULER_5WAVE: if (p->num_eqn != 5 || p->num_waves != 5) return CLAW2_ERR_INVALID; break;
     case CLAW2_RP_SHALLOW_ROE: if (p->num_eqn != 3 || p->num_waves != 3) return CLAW2_ERR_INVALID; break;
+    case CLAW2_RP_PSYSTEM: if (p->num_eqn != 3 || p->num_waves != 2 || p->num_aux < 4) return CLAW2_ERR_INVALID; break;
     default: return CLAW2_ERR_INVALID;
     }
     if (p->index_capa >= p->num_aux) return CLAW2_ERR_INVALID;

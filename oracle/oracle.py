@@ -161,7 +161,8 @@ class Run:
 
     def __init__(self, p, q, aux=None, *, cfl_max=1.0, cfl_desired=0.9, dt_initial=0.1,
                  dt_max=1e99, dt_variable=True, max_steps=10000, bc_callbacks=None,
-                 step_source=None, source_split=1, lib=None, omp=False):
+                 step_source=None, source_split=1, lib=None, omp=False, before_step=None,
+                 on_accept=None):
         self.p = p
         self.omp = omp
         self.lib = lib or load(omp)
@@ -181,6 +182,8 @@ class Run:
         self.bc_callbacks = bc_callbacks or {}
         self.step_source = step_source
         self.source_split = source_split
+        self.before_step = before_step      # f(run): may change the interior of run.auxbc
+        self.on_accept = on_accept          # f(run) after every accepted step (gauges)
         self.t = 0.0
         self.cfl = cfl_desired           # CFL(cfl_desired), solver.py:179
         self.status = {}
@@ -222,6 +225,9 @@ class Run:
 
     def step(self):
         """ClawSolver.step (classic/solver.py:100-151); returns True on success."""
+        if self.before_step is not None:            # classic/solver.py:128-129
+            self.before_step(self)
+            fill_aux_ghosts(self.p, self.auxbc, self.lib)    # apply_aux_bcs in step_hyperbolic
         self.apply_q_bcs()
         self.cfl = step_hyperbolic(self.p, self.qbc, self.auxbc, self.dt, lib=self.lib, omp=self.omp)
         g = self.p.num_ghost
@@ -272,6 +278,8 @@ class Run:
                     self.t = tstart + (n + 1) * self.dt
                 self.status["numsteps"] += 1
                 self.steps_taken += 1
+                if self.on_accept is not None:      # write_gauge_values, solver.py:654-656
+                    self.on_accept(self)
             else:
                 if self.dt_variable:
                     self.q = q_backup

@@ -30,6 +30,7 @@ RP_VC_ACOUSTICS = 2
 RP_EULER_4WAVE = 3
 RP_EULER_5WAVE = 4
 RP_SHALLOW_ROE = 5
+RP_PSYSTEM = 6
 
 # boundary conditions (enum claw2_bc == pyclaw.BC)
 BC_CUSTOM = 0
@@ -73,7 +74,8 @@ class Hooks(ctypes.Structure):
     _fields_ = [
         ("source", ctypes.c_int32),
         ("source_aux", ctypes.c_int32),
-        ("reserved_", ctypes.c_int32 * 2),
+        ("aux_from_q", ctypes.c_int32),
+        ("aux_q", ctypes.c_int32),
     ]
 
 

@@ -6,7 +6,8 @@ stays in GPU memory and the step is the fused sm_100a kernel of libclaw2.so.
 evolve_to_time runs the whole step-size control loop on the device (one kernel
 launch per step, no host round trip) unless a Python callback (before_step,
 step_source, a custom boundary condition) has to run between steps; the
-callbacks of pyclaw_b200.hooks run on the device, and gauges are sampled on
+callbacks of pyclaw_b200.hooks (FixedStateBC, EulerRadialSource, AuxFromQ)
+run on the device, and gauges are sampled on
 the device after every accepted step and written out after each batch of
 steps.
 """
@@ -220,8 +221,15 @@ class ClawSolver2D(ClawSolver):
         """The claw2_hooks that let the device run this solver's callbacks
         itself (hooks.EulerRadialSource, hooks.FixedStateBC), or None when
         some callback has to run on the host."""
-        from .hooks import EulerRadialSource, FixedStateBC
+        from .hooks import AuxFromQ, EulerRadialSource, FixedStateBC
         h = _abi.Hooks()
+        if self.before_step is not None:
+            if not isinstance(self.before_step, AuxFromQ):
+                return None
+            if list(self.aux_bc_lower) != list(self.bc_lower) or list(self.aux_bc_upper) != list(self.bc_upper):
+                return None
+            h.aux_from_q = self.before_step.aux_index + 1
+            h.aux_q = self.before_step.q_index + 1
         if self.step_source is not None:
             if not isinstance(self.step_source, EulerRadialSource) or self.source_split != 1:
                 return None
@@ -233,7 +241,7 @@ class ClawSolver2D(ClawSolver):
         return h
 
     def _device_loop_ok(self, solution):
-        return self.before_step is None and self._device_hooks() is not None
+        return self._device_hooks() is not None
 
     def evolve_to_time(self, solution, tend=None):
         if not self._is_set_up:
@@ -256,7 +264,7 @@ class ClawSolver2D(ClawSolver):
         if not self.dt_variable:
             self.max_steps = int(c.max_steps)
         hooks = None
-        if self.step_source is not None or self._custom_bcs():
+        if self.step_source is not None or self._custom_bcs() or self.before_step is not None:
             hooks = self._device_hooks()
             if self._custom_bcs():
                 # fixed-state sides: set once in both state buffers; the

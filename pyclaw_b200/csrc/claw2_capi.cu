@@ -165,12 +165,15 @@ batch_kernel(const claw2_batch_instance* __restrict__ inst, int ninst, int ntile
         for (int i = threadIdx.x; i < ninst; i += NT) tb[i] = __ldg(&inst[i].tile_begin);
         __syncthreads();
     }
+    // each CTA takes a contiguous run of tiles: consecutive tiles mostly
+    // belong to the same instance (its descriptor and controller stay in L1)
+    // and share halo lines with the tile before them
+    const int tbeg = (int)((long long)ntiles * blockIdx.x / gridDim.x);
+    const int tend = (int)((long long)ntiles * (blockIdx.x + 1) / gridDim.x);
     int next = -1;                                  // instance of the next tile, found by its prefetch
-    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    for (int t = tbeg; t < tend; t++) {
         const int lo = next >= 0 ? next : batch_instance_of(inst, ninst, t, tb);
-        next = t + (int)gridDim.x < ntiles
-                   ? batch_prefetch_tile<RP::MEQN, RP::MAUX, T, T, NT>(inst, ninst, t + (int)gridDim.x, tb)
-                   : -1;
+        next = t + 1 < tend ? batch_prefetch_tile<RP::MEQN, RP::MAUX, T, T, NT>(inst, ninst, t + 1, tb) : -1;
         const claw2_batch_instance& I = inst[lo];
         StepArgs a = common;
         a.q0 = I.q0; a.q1 = I.q1; a.aux = I.aux; a.ctrl = I.ctrl;
@@ -314,6 +317,18 @@ __global__ void halo_kernel(double* q0, double* q1, const claw2_control* c, doub
     }
 }
 
+// Before-step copy of plane `from` of q[cur] (ghost cells included) into
+// plane `to` of aux (claw2_hooks.aux_from_q).
+__global__ void aux_from_q_kernel(double* aux, const double* q0, const double* q1, const claw2_control* c,
+                                  long long plane, int from, int to)
+{
+    if (c->done) return;
+    const double* q = (c->cur ? q1 : q0) + (long long)from * plane;
+    double* d = aux + (long long)to * plane;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < plane; t += (long long)gridDim.x * blockDim.x)
+        d[t] = q[t];
+}
+
 // Gauge samples after a step (claw2_gauges): one block; nothing happens
 // unless the controller accepted a step since the last row.
 __global__ void gauge_record_kernel(claw2_gauges g, const double* q0, const double* q1, const claw2_control* c,
@@ -368,6 +383,7 @@ int solver_shape(int rp, int* meqn, int* mw, int* maux)
     case CLAW2_RP_EULER_4WAVE: *meqn = 4; *mw = 4; *maux = 0; return 0;
     case CLAW2_RP_EULER_5WAVE: *meqn = 5; *mw = 5; *maux = 0; return 0;
     case CLAW2_RP_SHALLOW_ROE: *meqn = 3; *mw = 3; *maux = 0; return 0;
+    case CLAW2_RP_PSYSTEM: *meqn = 3; *mw = 2; *maux = 4; return 0;
     default: return -1;
     }
 }
@@ -527,6 +543,8 @@ int launch_step(const claw2_problem* p, const StepArgs& a, cudaStream_t st)
         return split ? launch_step_t<RpEuler<true>, true>(a, nbx, nby, st) : launch_step_t<RpEuler<true>, false>(a, nbx, nby, st);
     case CLAW2_RP_SHALLOW_ROE:
         return split ? launch_step_t<RpShallow, true>(a, nbx, nby, st) : launch_step_t<RpShallow, false>(a, nbx, nby, st);
+    case CLAW2_RP_PSYSTEM:
+        return split ? launch_step_t<RpPsystem, true>(a, nbx, nby, st) : launch_step_t<RpPsystem, false>(a, nbx, nby, st);
     default:
         return CLAW2_ERR_INVALID;
     }
@@ -705,25 +723,58 @@ int claw2_advance(const claw2_problem* p, double* q0, double* q1, const double* 
     return CLAW2_OK;
 }
 
+}  // extern "C"
+
+namespace {
+// Checks claw2_hooks against the problem and sets the source term in a.
+int apply_hooks(const claw2_problem* p, const claw2_hooks* hooks, StepArgs& a)
+{
+    if (hooks->source != CLAW2_SRC_NONE && hooks->source != CLAW2_SRC_EULER_RADIAL) return CLAW2_ERR_INVALID;
+    if (hooks->source == CLAW2_SRC_EULER_RADIAL &&
+        ((p->rp != CLAW2_RP_EULER_4WAVE && p->rp != CLAW2_RP_EULER_5WAVE) || hooks->source_aux < 0 ||
+         hooks->source_aux >= p->num_aux))
+        return CLAW2_ERR_UNSUPPORTED;
+    if (hooks->aux_from_q != 0) {
+        const int k = hooks->aux_from_q - 1, m = hooks->aux_q - 1;
+        if (k < 0 || k >= p->num_aux || m < 0 || m >= p->num_eqn) return CLAW2_ERR_INVALID;
+        for (int d = 0; d < 2; d++)
+            if (p->aux_bc_lower[d] != p->bc_lower[d] || p->aux_bc_upper[d] != p->bc_upper[d] ||
+                p->bc_lower[d] == CLAW2_BC_CUSTOM || p->bc_upper[d] == CLAW2_BC_CUSTOM)
+                return CLAW2_ERR_UNSUPPORTED;
+    }
+    a.src = hooks->source;
+    a.src_aux = hooks->source_aux;
+    return CLAW2_OK;
+}
+
+int launch_aux_from_q(const claw2_hooks* hooks, const StepArgs& a, double* aux, double* q0, double* q1,
+                      claw2_control* ctrl, cudaStream_t st)
+{
+    if (!hooks || hooks->aux_from_q == 0) return CLAW2_OK;
+    const long long n = a.plane;
+    int blocks = (int)((n + 255) / 256);
+    if (blocks > 148 * 8) blocks = 148 * 8;
+    aux_from_q_kernel<<<blocks, 256, 0, st>>>(aux, q0, q1, ctrl, a.plane, hooks->aux_q - 1, hooks->aux_from_q - 1);
+    return cudaGetLastError() == cudaSuccess ? CLAW2_OK : CLAW2_ERR_CUDA;
+}
+}  // namespace
+
+extern "C" {
+
 int claw2_advance_hooked(const claw2_problem* p, double* q0, double* q1, const double* aux, claw2_control* ctrl,
                          void* scratch, int nsteps, const claw2_hooks* hooks, void* stream)
 {
     int rc = claw2_validate(p);
     if (rc) return rc;
     if (!q0 || !q1 || !ctrl || !scratch || !hooks || (p->num_aux > 0 && !aux) || nsteps < 0) return CLAW2_ERR_INVALID;
-    if (hooks->source != CLAW2_SRC_NONE && hooks->source != CLAW2_SRC_EULER_RADIAL) return CLAW2_ERR_INVALID;
-    if (hooks->source == CLAW2_SRC_EULER_RADIAL &&
-        ((p->rp != CLAW2_RP_EULER_4WAVE && p->rp != CLAW2_RP_EULER_5WAVE) || hooks->source_aux < 0 ||
-         hooks->source_aux >= p->num_aux))
-        return CLAW2_ERR_UNSUPPORTED;
     StepArgs a;
     fill_args(p, q0, a);
     a.q0 = q0; a.q1 = q1; a.aux = aux; a.ctrl = ctrl;
     a.ticket = static_cast<unsigned int*>(scratch);
     a.partials = reinterpret_cast<double*>(static_cast<char*>(scratch) + 64);
-    a.src = hooks->source;
-    a.src_aux = hooks->source_aux;
+    if ((rc = apply_hooks(p, hooks, a))) return rc;
     for (int n = 0; n < nsteps; n++) {
+        if ((rc = launch_aux_from_q(hooks, a, const_cast<double*>(aux), q0, q1, ctrl, S(stream)))) return rc;
         if ((rc = launch_step(p, a, S(stream)))) return rc;
         if (!a.ghost_fused &&
             (rc = launch_fill(p, nullptr, p->num_eqn, p->bc_lower, p->bc_upper, false, q0, q1, ctrl, S(stream))))
@@ -744,17 +795,10 @@ int claw2_advance_gauged(const claw2_problem* p, double* q0, double* q1, const d
     a.q0 = q0; a.q1 = q1; a.aux = aux; a.ctrl = ctrl;
     a.ticket = static_cast<unsigned int*>(scratch);
     a.partials = reinterpret_cast<double*>(static_cast<char*>(scratch) + 64);
-    if (hooks) {
-        if (hooks->source != CLAW2_SRC_NONE && hooks->source != CLAW2_SRC_EULER_RADIAL) return CLAW2_ERR_INVALID;
-        if (hooks->source == CLAW2_SRC_EULER_RADIAL &&
-            ((p->rp != CLAW2_RP_EULER_4WAVE && p->rp != CLAW2_RP_EULER_5WAVE) || hooks->source_aux < 0 ||
-             hooks->source_aux >= p->num_aux))
-            return CLAW2_ERR_UNSUPPORTED;
-        a.src = hooks->source;
-        a.src_aux = hooks->source_aux;
-    }
+    if (hooks && (rc = apply_hooks(p, hooks, a))) return rc;
     const int threads = 128;
     for (int n = 0; n < nsteps; n++) {
+        if ((rc = launch_aux_from_q(hooks, a, const_cast<double*>(aux), q0, q1, ctrl, S(stream)))) return rc;
         if ((rc = launch_step(p, a, S(stream)))) return rc;
         if (!a.ghost_fused &&
             (rc = launch_fill(p, nullptr, p->num_eqn, p->bc_lower, p->bc_upper, false, q0, q1, ctrl, S(stream))))
@@ -954,6 +998,7 @@ int batch_launch(const claw2_problem* p, const claw2_batch_instance* inst, int n
     case CLAW2_RP_EULER_4WAVE: return batch_launch_rp<RpEuler<false>>(variant, c, inst, ninst, ntiles, nsteps, st);
     case CLAW2_RP_EULER_5WAVE: return batch_launch_rp<RpEuler<true>>(variant, c, inst, ninst, ntiles, nsteps, st);
     case CLAW2_RP_SHALLOW_ROE: return batch_launch_rp<RpShallow>(variant, c, inst, ninst, ntiles, nsteps, st);
+    case CLAW2_RP_PSYSTEM: return batch_launch_rp<RpPsystem>(variant, c, inst, ninst, ntiles, nsteps, st);
     default: return CLAW2_ERR_INVALID;
     }
 }

@@ -563,4 +563,67 @@ struct RpShallow {
     }
 };
 
+// ---------------------------------------------------------------------------
+// Two-dimensional p-system with f-waves (nonlinear elasticity in layered
+// media, apps/psystem_2d/psystem.py): q = (eps, rho u, rho v), aux = (rho, K,
+// linearity, eps of the cell before the step); sigma = K eps (linearity 1) or
+// exp(K eps) - 1 (linearity 2), c = sqrt(sigma_eps / rho), Z = rho c.  The
+// normal solve splits the flux jump of f = (-u, -sigma, 0) on (1, Z_left) with
+// speed -c_left and (1, -Z_right) with speed c_right; the transverse solve
+// splits a fluctuation on (1, Z_below) going down with -c_below and
+// (1, -Z_above) going up with c_above.  Same formulas as the oracle.
+// ---------------------------------------------------------------------------
+struct RpPsystem {
+    static constexpr int MEQN = 3, MW = 2, MAUX = 4, NROE = 1;
+
+    static CLAW2_DEV void cell(const double* aux, double eps, double& sigma, double& c, double& z)
+    {
+        const double rho = aux[0], K = aux[1];
+        double se;
+        if (aux[2] == 1.0) { sigma = K * eps; se = K; }
+        else { const double e = exp(K * eps); sigma = e - 1.0; se = K * e; }
+        c = sqrt(se / rho);
+        z = rho * c;
+    }
+
+    template <int IXY>
+    static CLAW2_DEV void rpn2(const double (&qL)[MEQN], const double (&qR)[MEQN],
+                                                const double* auxL, const double* auxR, const double*,
+                                                double (&wave)[MW][MEQN], double (&s)[MW],
+                                                double (&amdq)[MEQN], double (&apdq)[MEQN],
+                                                double (&)[NROE])
+    {
+        constexpr int mu = Dir<IXY>::MU, mv = Dir<IXY>::MV;
+        double sgl, cl, zl, sgr, cr, zr;
+        cell(auxL, qL[0], sgl, cl, zl);
+        cell(auxR, qR[0], sgr, cr, zr);
+        const double ul = qL[mu] / auxL[0];
+        const double ur = qR[mu] / auxR[0];
+        const double df1 = (-ur) - (-ul);
+        const double df2 = (-sgr) - (-sgl);
+        const double b1 = (zr * df1 + df2) / (zl + zr);
+        const double b2 = (zl * df1 - df2) / (zl + zr);
+        wave[0][0] = b1; wave[0][mu] = b1 * zl; wave[0][mv] = 0.0; s[0] = -cl;
+        wave[1][0] = b2; wave[1][mu] = -b2 * zr; wave[1][mv] = 0.0; s[1] = cr;
+#pragma unroll
+        for (int m = 0; m < MEQN; m++) { amdq[m] = wave[0][m]; apdq[m] = wave[1][m]; }
+    }
+
+    // a1p/a3p: aux of the cells below and above the one the fluctuation sits in
+    template <int IXY>
+    static CLAW2_DEV void rpt2(int, const double (&asdq)[MEQN], const double (&)[NROE],
+                                                const double* a1p, const double*, const double* a3p,
+                                                const double*, double (&bm)[MEQN], double (&bp)[MEQN])
+    {
+        constexpr int mu = Dir<IXY>::MU, mv = Dir<IXY>::MV;
+        double sgb, cb, zb, sga, ca, za;
+        cell(a1p, a1p[3], sgb, cb, zb);
+        cell(a3p, a3p[3], sga, ca, za);
+        const double gb = (za * asdq[0] + asdq[mv]) / (zb + za);
+        const double ga = (zb * asdq[0] - asdq[mv]) / (zb + za);
+        bm[0] = -cb * gb; bm[mu] = 0.0; bm[mv] = -cb * gb * zb;
+        bp[0] = ca * ga; bp[mu] = 0.0; bp[mv] = -ca * ga * za;
+    }
+};
+
 }  // namespace claw2

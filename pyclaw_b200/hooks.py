@@ -15,6 +15,10 @@ evolve_to_time loop on the device:
   equations with radial symmetry, two-stage Runge-Kutta
   (apps/euler_2d/shockbubble.py:89-124), fused into the step kernel.  Used
   with Godunov splitting (solver.source_split = 1).
+* ``AuxFromQ(aux_index=3, q_index=0)``: a before_step callback that copies a
+  state component into an aux component the Riemann solver reads, like the
+  p-system app's b4step (apps/psystem_2d/psystem.py:86-90, aux[3] = q[0] for
+  its transverse solver); on the device a copy kernel runs before each step.
 """
 import numpy as np
 
@@ -76,3 +80,17 @@ class EulerRadialSource(object):
         q[1, :, :] = q[1, :, :] - dt * (ndim - 1) / rad * rho * u * v
         q[2, :, :] = q[2, :, :] - dt * (ndim - 1) / rad * rho * v * v
         q[3, :, :] = q[3, :, :] - dt * (ndim - 1) / rad * v * (qstar[3, :, :] + press)
+
+
+class AuxFromQ(object):
+    """before_step(solver, state): state.aux[aux_index] = state.q[q_index].
+    On the device loop the copy runs before every step, ghost cells included,
+    which needs the aux boundary conditions of that component to equal those
+    of q (ClawSolver2D falls back to the host loop otherwise)."""
+
+    def __init__(self, aux_index=3, q_index=0):
+        self.aux_index = int(aux_index)
+        self.q_index = int(q_index)
+
+    def __call__(self, solver, state):
+        state.aux[self.aux_index, :, :] = state.q[self.q_index, :, :]

@@ -39,8 +39,13 @@ rp2_euler_5wave = RiemannSolver('rp2_euler_5wave', _abi.RP_EULER_5WAVE, 5, 5, 0,
 rp2_shallow_roe_with_efix = RiemannSolver('rp2_shallow_roe_with_efix', _abi.RP_SHALLOW_ROE, 3, 3, 0,
                                           ('grav',))
 
+# f-wave solver (set solver.fwave = True, as apps/psystem_2d/psystem.py does);
+# aux = (rho, K, linearity, eps), the application copies q[0] into aux[3]
+# before each step
+rp2_psystem = RiemannSolver('rp2_psystem', _abi.RP_PSYSTEM, 3, 2, 4, ())
+
 SOLVERS = {s.name: s for s in (rp2_acoustics, rp2_vc_acoustics, rp2_euler_4wave, rp2_euler_5wave,
-                               rp2_shallow_roe_with_efix)}
+                               rp2_shallow_roe_with_efix, rp2_psystem)}
 
 
 class static(object):

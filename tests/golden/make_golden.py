@@ -18,6 +18,9 @@ without the reference tree being present:
                             fort.q0020 (q, 3x200x200), fort.a0000 (aux, 2x200x200)
                             and the fort.t headers (test_acoustics_2d_variable_io.py,
                             reltol 1e-4)
+  psystem_gauges.npz        apps/psystem_2d/verify_gauge<x>_<y>.txt, the four
+                            gauges' (t, p, 10 p) rows (test_2d_psystem.py:9-30,
+                            reltol 1e-4)
 
 Usage: python tests/golden/make_golden.py /path/to/reference
    or: CLAW2_REFERENCE=/path/to/reference python tests/golden/make_golden.py
@@ -45,7 +48,18 @@ def read_fort(path, nvar):
     return np.ascontiguousarray(np.transpose(a, (2, 1, 0)))   # -> (m, i, j)
 
 
+PSYSTEM_GAUGES = ("0.25_0.25", "17.85_1.25", "3.25_18.75", "11.75_11.75")
+
+
+def psystem(ref):
+    apps = os.path.join(ref, "apps")
+    g = {"g" + k.replace(".", "p"): np.loadtxt(os.path.join(apps, "psystem_2d", "verify_gauge%s.txt" % k))
+         for k in PSYSTEM_GAUGES}
+    np.savez_compressed(os.path.join(HERE, "psystem_gauges.npz"), **g)
+
+
 def main(ref):
+    psystem(ref)
     apps = os.path.join(ref, "apps")
     d = np.loadtxt(os.path.join(apps, "euler_2d", "verify_shockbubble_classic.txt"))
     np.savez_compressed(os.path.join(HERE, "shockbubble_density.npz"), density=d)

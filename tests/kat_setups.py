@@ -177,3 +177,75 @@ def check_diff(expected, test, **kw):
     if "reltol" in kw:
         return None if err_norm / expected_norm < kw["reltol"] else (expected_norm, test_norm, err_norm)
     raise Exception('Incorrect use of check_diff verifier, specify tol!')
+
+
+# --------------------------------------------------------------------------
+# apps/psystem_2d/psystem.py (:12-90 and psystem2D, :118-233; classic solver)
+# --------------------------------------------------------------------------
+PSYSTEM_GAUGES = [[0.25, 0.25], [17.85, 1.25], [3.25, 18.75], [11.75, 11.75]]
+
+
+def psystem_setup():
+    """Checkerboard of two nonlinear (exponential) materials, rho and E of 1
+    and 4 in cells of 0.5; sigma(t=0) = 10 exp(-(x-0.25)^2 - (y-0.25)^2) at the
+    walled corner; f-waves, superbee, unsplit with transverse_waves = 1 (the
+    ClawSolver2D default), cfl 0.8/0.9, walls at the lower and extrapolation
+    at the upper boundaries, t = 40 in 10 output intervals.  Returns (problem,
+    q0, aux0 (aux[3] = q[0]), run settings, gauge cell indices)."""
+    E1, p1, E2, p2 = 1., 1., 4., 4.
+    x_lower, x_upper = 0.25, 20.25
+    mx = my = int((x_upper - x_lower) * 10)
+    x, dx = centers(x_lower, x_upper, mx)
+    y, dy = centers(x_lower, x_upper, my)
+    xfrac = x - np.floor(x / 1.0) * 1.0
+    yfrac = y - np.floor(y / 1.0) * 1.0
+    yyfrac, xxfrac = np.meshgrid(yfrac, xfrac)
+    a = (xxfrac <= 0.5) * (yyfrac <= 0.5)
+    b = (xxfrac > 0.5) * (yyfrac > 0.5)
+    c = (xxfrac > 0.5) * (yyfrac <= 0.5)
+    d = (xxfrac <= 0.5) * (yyfrac > 0.5)
+    aux = np.empty((4, mx, my), order="F")
+    aux[0] = p1 * a + p1 * b + p2 * c + p2 * d
+    aux[1] = E1 * a + E1 * b + E2 * c + E2 * d
+    aux[2] = 2 * a + 2 * b + 2 * c + 2 * d
+    yy, xx = np.meshgrid(y, x)
+    s = 10. * np.exp(-(xx - 0.25) ** 2 / (2 * 0.5) - (yy - 0.25) ** 2 / (2 * 0.5))
+    q = np.empty((3, mx, my), order="F")
+    q[0] = np.where(aux[2] == 1, 1, 0) * s / aux[1] + np.where(aux[2] == 2, 1, 0) * np.log(s + 1) / aux[1]
+    q[1] = 0.
+    q[2] = 0.
+    aux[3] = q[0]
+    p = _abi.make_problem(rp=_abi.RP_PSYSTEM, num_eqn=3, num_waves=2, num_aux=4, mx=mx, my=my, dx=dx, dy=dy,
+                          order=2, transverse=1, mthlim=[2], use_fwave=True,
+                          bc_lower=(_abi.BC_WALL, _abi.BC_WALL), bc_upper=(_abi.BC_EXTRAP, _abi.BC_EXTRAP),
+                          aux_bc_lower=(_abi.BC_WALL, _abi.BC_WALL),
+                          aux_bc_upper=(_abi.BC_EXTRAP, _abi.BC_EXTRAP))
+    run = dict(cfl_max=0.9, cfl_desired=0.8, dt_initial=0.1)
+    gauges = [[int(round((g[n] - x_lower) / dx)) for n in range(2)] for g in PSYSTEM_GAUGES]
+    return p, q, aux, run, gauges
+
+
+def psystem_gauge_values(q, aux):
+    """gauge_pfunction of the app (:107-109): p = exp(eps E) - 1, and 10 p."""
+    p = np.exp(q[0] * aux[1]) - 1
+    return [p, 10 * p]
+
+
+def psystem_oracle_run(orc, omp=True):
+    """The app through the oracle: before every step aux[3] = q[0] (b4step,
+    :86-90), gauges written at t = 0 and after every accepted step.  Returns
+    the four gauges' (t, p, 10 p) rows and the final run."""
+    p, q, aux, run, gauges = psystem_setup()
+    rows = [[] for _ in gauges]
+
+    def b4step(r):
+        r.auxbc[3, 2:-2, 2:-2] = r.q[0]
+
+    def record(r):
+        for k, (ix, iy) in enumerate(gauges):
+            rows[k].append([r.t] + psystem_gauge_values(r.q[:, ix, iy], r.auxbc[:, ix + 2, iy + 2]))
+
+    r = orc.Run(p, q, aux, before_step=b4step, on_accept=record, omp=omp, **run)
+    record(r)
+    r.run(40.0, num_output_times=10, keep_copy=False)
+    return [np.array(g) for g in rows], r

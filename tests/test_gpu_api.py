@@ -397,3 +397,69 @@ def test_gauges_recorded_on_the_device(orc, tmp_path):
         qg = frames[-1][:, ix, iy]
         assert st_d.gauge_data[i][-1][0] == ref.t
         assert list(st_d.gauge_data[i][-1][1:]) == [qg[0] * aux[0, ix, iy], qg[1] + qg[2]]
+
+
+def _psystem_api_run(before_step, outdir):
+    """apps/psystem_2d/psystem.py:118-233 through the public API."""
+    p, q, aux, run, gauges = K.psystem_setup()
+    x = pc.Dimension('x', 0.25, 20.25, p.mx)
+    y = pc.Dimension('y', 0.25, 20.25, p.my)
+    domain = pc.Domain([x, y])
+    state = pc.State(domain, 3, 4)
+    state.aux[...] = aux
+    state.q[...] = q
+    state.keep_gauges = True
+    state.grid.add_gauges(K.PSYSTEM_GAUGES)
+    assert [list(g) for g in state.grid.gauges] == gauges
+    solver = pc.ClawSolver2D(pc.riemann.rp2_psystem)
+    solver.limiters = pc.limiters.tvd.superbee
+    solver.bc_lower = [pc.BC.wall, pc.BC.wall]
+    solver.bc_upper = [pc.BC.extrap, pc.BC.extrap]
+    solver.aux_bc_lower = [pc.BC.wall, pc.BC.wall]
+    solver.aux_bc_upper = [pc.BC.extrap, pc.BC.extrap]
+    solver.fwave = True
+    solver.cfl_max = 0.9
+    solver.cfl_desired = 0.8
+    solver.before_step = before_step
+    solver.dimensional_split = False
+    solver.compute_gauge_values = K.psystem_gauge_values
+    claw = pc.Controller()
+    claw.tfinal = 40.0
+    claw.solver = solver
+    claw.outdir = outdir
+    claw.solution = pc.Solution(state, domain)
+    claw.num_output_times = 10
+    claw.output_format = None
+    claw.run()
+    return claw, solver, state
+
+
+def test_psystem_fwave_app_matches_reference_gauges(orc, tmp_path):
+    """apps/psystem_2d/test_2d_psystem.py on the GPU: the f-wave p-system with
+    its before-step copy of eps into aux (hooks.AuxFromQ, a copy kernel
+    before every step) and its four gauges (recorded on the device), the
+    whole 40-time-unit run in the device loop.  Gauges against the
+    reference's verify_gauge*.txt at its reltol 1e-4 (reached: 1e-10), against
+    the oracle's run to 1e-11 relative (the solver calls exp, whose last bit
+    may differ between the host's and the device's libraries), and the same
+    app with the copy as a Python callback (host loop) is bit-identical."""
+    claw, solver, state = _psystem_api_run(pc.hooks.AuxFromQ(3, 0), str(tmp_path / "dev"))
+    assert solver._device_loop_ok(claw.solution)
+    gold = np.load(os.path.join(GOLD, "psystem_gauges.npz"))
+    rows, r = K.psystem_oracle_run(orc)
+    for i, key in enumerate(("g0p25_0p25", "g17p85_1p25", "g3p25_18p75", "g11p75_11p75")):
+        got = np.asarray(state.gauge_data[i])
+        assert got.shape == gold[key].shape, (key, got.shape)
+        assert K.check_diff(gold[key], got, reltol=1e-4) is None, key
+        assert np.linalg.norm(gold[key] - got) / np.linalg.norm(gold[key]) < 1e-10, key
+        assert np.max(np.abs(got - rows[i])) <= 1e-11 * np.max(np.abs(rows[i])), key
+    scale = np.max(np.abs(r.q), axis=(1, 2))
+    assert np.all(np.max(np.abs(state.q - r.q), axis=(1, 2)) <= 1e-11 * scale)
+
+    def b4step(s, st):
+        st.aux[3, :, :] = st.q[0, :, :]
+    claw_h, solver_h, state_h = _psystem_api_run(b4step, str(tmp_path / "host"))
+    assert not solver_h._device_loop_ok(claw_h.solution)
+    for gd, gh in zip(state.gauge_data, state_h.gauge_data):
+        assert np.array_equal(gd, gh)
+    assert np.array_equal(state.q, state_h.q)

@@ -6,6 +6,7 @@ through the oracle and applies the reference test's own comparison:
   apps/acoustics_2d_homogeneous/test_2d_acoustics.py:115-116   reltol 1e-3
   apps/acoustics_2d_variable/test_acoustics_2d_variable.py:111-115  max-abs 0.1
   apps/acoustics_2d_variable/test_acoustics_2d_variable_io.py:146-182 reltol 1e-4
+  apps/psystem_2d/test_2d_psystem.py:9-30 (gauges, f-waves)        reltol 1e-4
 """
 import os
 
@@ -67,3 +68,18 @@ def test_omp_gather_form_is_bit_identical(orc):
             assert ca == cb
             g = p.num_ghost
             assert np.array_equal(a[:, g:-g, g:-g], b[:, g:-g, g:-g])
+
+
+def test_psystem_fwave_gauges_match_reference(orc):
+    """apps/psystem_2d/test_2d_psystem.py: the f-wave p-system with its
+    before-step copy of eps into aux, gauges written after every accepted
+    step; each gauge's (t, p, 10 p) rows against verify_gauge*.txt at reltol
+    1e-4 (the restated solver reaches the files' printed digits)."""
+    rows, r = K.psystem_oracle_run(orc)
+    gold = np.load(os.path.join(GOLD, "psystem_gauges.npz"))
+    for got, key in zip(rows, ("g0p25_0p25", "g17p85_1p25", "g3p25_18p75", "g11p75_11p75")):
+        exp = gold[key]
+        assert got.shape == exp.shape, (key, got.shape, exp.shape)
+        assert K.check_diff(exp, got, reltol=1e-4) is None, key
+        assert np.linalg.norm(exp - got) / np.linalg.norm(exp) < 1e-10, key
+    assert abs(r.t - 40.0) < 1e-12
