@@ -112,21 +112,30 @@ __device__ __forceinline__ int batch_instance_of(const claw2_batch_instance* __r
 // shared memory (4 bytes each)
 constexpr int kBatchTableMax = 4096;
 
-// Ask L2 for the input halo of tile t (rows j0-2..j0+TY+1 and columns
-// i0-2..i0+TX+1, clipped to the ghosted arrays, of the current state and of
-// aux) while the CTA works on the tile before it: an instance's data is read
-// once per step, from HBM, so the tile's first loads would otherwise wait for
-// DRAM.  One prefetch per 128-byte line, spread over the CTA's threads.  The
-// addresses stay inside the instance's arrays; results do not depend on it.
-// Returns tile t's instance.
-template <int MEQN, int MAUX, int TX, int TY, int NT>
-__device__ __forceinline__ int batch_prefetch_tile(const claw2_batch_instance* __restrict__ inst, int ninst, int t,
-                                                   const int* tb)
+// Instance of tile t + 1 given k, the instance of tile t: tile_begin is
+// non-decreasing, so it is the last instance at or after k whose tile_begin is
+// <= t + 1 (the same one or, crossing an instance's last tile, the next one
+// with tiles).
+__device__ __forceinline__ int batch_instance_after(const claw2_batch_instance* __restrict__ inst, int ninst, int k,
+                                                    int t, const int* tb)
 {
-    const int k = batch_instance_of(inst, ninst, t, tb);
+    while (k + 1 < ninst && (tb ? tb[k + 1] : __ldg(&inst[k + 1].tile_begin)) <= t + 1) k++;
+    return k;
+}
+
+// Ask L2 for the input halo of tile t (instance k; rows j0-2..j0+TY+1 and
+// columns i0-2..i0+TX+1, clipped to the ghosted arrays, of the current state
+// and of aux) while the CTA works on the tile before it: an instance's data is
+// read once per step, from HBM, so the tile's first loads would otherwise wait
+// for DRAM.  One prefetch per 128-byte line, spread over the CTA's threads.
+// The addresses stay inside the instance's arrays; results do not depend on
+// it.
+template <int MEQN, int MAUX, int TX, int TY, int NT>
+__device__ __forceinline__ void batch_prefetch_tile(const claw2_batch_instance* __restrict__ inst, int k, int t)
+{
     const claw2_batch_instance& I = inst[k];
     const claw2_control* c = I.ctrl;
-    if (c->done) return k;
+    if (c->done) return;
     const double* q = c->cur ? I.q1 : I.q0;
     const int lt = t - I.tile_begin;
     const int i0 = (lt % I.nbx) * TX, j0 = (lt / I.nbx) * TY;
@@ -143,7 +152,6 @@ __device__ __forceinline__ int batch_prefetch_tile(const claw2_batch_instance* _
         const char* row = base + (long long)(rlo + r + CLAW2_NUM_GHOST) * I.ld * 8 + ((long long)l0 << 7);
         for (int line = 0; line < nl; line++) asm volatile("prefetch.global.L2 [%0];" ::"l"(row + (line << 7)));
     }
-    return k;
 }
 
 // Batched step: a persistent grid walks the concatenated tile list of all
@@ -170,10 +178,11 @@ batch_kernel(const claw2_batch_instance* __restrict__ inst, int ninst, int ntile
     // and share halo lines with the tile before them
     const int tbeg = (int)((long long)ntiles * blockIdx.x / gridDim.x);
     const int tend = (int)((long long)ntiles * (blockIdx.x + 1) / gridDim.x);
-    int next = -1;                                  // instance of the next tile, found by its prefetch
+    // the run's first instance by binary search, then one step at a time
+    int lo = tbeg < tend ? batch_instance_of(inst, ninst, tbeg, tb) : 0;
     for (int t = tbeg; t < tend; t++) {
-        const int lo = next >= 0 ? next : batch_instance_of(inst, ninst, t, tb);
-        next = t + 1 < tend ? batch_prefetch_tile<RP::MEQN, RP::MAUX, T, T, NT>(inst, ninst, t + 1, tb) : -1;
+        const int nxt = t + 1 < tend ? batch_instance_after(inst, ninst, lo, t, tb) : lo;
+        if (t + 1 < tend) batch_prefetch_tile<RP::MEQN, RP::MAUX, T, T, NT>(inst, nxt, t + 1);
         const claw2_batch_instance& I = inst[lo];
         StepArgs a = common;
         a.q0 = I.q0; a.q1 = I.q1; a.aux = I.aux; a.ctrl = I.ctrl;
@@ -185,6 +194,7 @@ batch_kernel(const claw2_batch_instance* __restrict__ inst, int ninst, int ntile
         if constexpr (LIGHT) light_tile_at<RP, T, T, NT>(a, ctx, tile);
         else step_tile_at<RP, 29, 29, NT, false>(a, ctx, tile);
         __syncthreads();                            // shared memory is reused by the next tile
+        lo = nxt;
     }
 }
 
