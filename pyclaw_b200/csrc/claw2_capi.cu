@@ -72,16 +72,20 @@ template <> struct HasLean<RpEuler<false>> { static constexpr bool value = true;
 template <> struct HasLean<RpEuler<true>> { static constexpr bool value = true; };
 template <> struct HasLean<RpShallow> { static constexpr bool value = true; };
 
-#ifndef CLAW2_LEAN_MINB
-#define CLAW2_LEAN_MINB 2
-#endif
-// lean tiles: 28 x 28 cells, so that a line's 32 lanes hold its 32 cells
+// lean tiles: 28 x 28 cells, so that a line's 32 lanes hold its 32 cells.
+// Two block sizes, one line of a chunk per warp: 512 threads (one CTA per SM,
+// 16 lines per chunk) halve a tile's latency, which decides the step when the
+// grid has few tiles per SM (a launch of a few waves ends with a partial
+// one); 256 threads (two CTAs per SM) let one CTA's waits (its halo copy, its
+// barriers, the launch of the next CTA) overlap the other's work, which
+// decides it when the grid has many tiles, most of them cheap.
 constexpr int LTX = 28, LTY = 28;
+constexpr int LEAN_BIG_BLOCK_TILES = 8 * 148;   // grids of at most 8 tiles per SM of a B200 use 512 threads
 
 // tm0 / tm1: tensor maps of the input state (see lean_tile_at), passed as
 // __grid_constant__ parameters so the TMA unit can read them in place.
-template <class RP>
-__global__ void __launch_bounds__(256, CLAW2_LEAN_MINB)
+template <class RP, int NT>
+__global__ void __launch_bounds__(NT, 512 / NT)
 lean_step_kernel(StepArgs a, const __grid_constant__ CUtensorMap tm0, const __grid_constant__ CUtensorMap tm1)
 {
     extern __shared__ double smem_dyn[];
@@ -89,7 +93,7 @@ lean_step_kernel(StepArgs a, const __grid_constant__ CUtensorMap tm0, const __gr
     DevCtx ctx{smem_dyn};
     const TileId t{(int)blockIdx.x, (int)blockIdx.y, (int)gridDim.x, (int)gridDim.y,
                    (int)(blockIdx.y * gridDim.x + blockIdx.x), (int)(gridDim.x * gridDim.y)};
-    lean_tile_at<RP, LTX, LTY, 256>(a, ctx, t, &tm0, &tm1, &halo_bar);
+    lean_tile_at<RP, LTX, LTY, NT>(a, ctx, t, &tm0, &tm1, &halo_bar);
 }
 
 // Instance of tile t: the last one with tile_begin <= t (binary search).
@@ -409,6 +413,14 @@ bool fused_ghosts(const claw2_problem* p)
     return p->mx >= 4 && p->my >= 4;
 }
 
+// Problems stepped by the lean body (launch_step_t): unsplit Euler and
+// shallow water without capacity or f-waves.
+bool lean_body(const claw2_problem* p)
+{
+    return p->transverse >= 0 && p->index_capa < 0 && !p->use_fwave &&
+           (p->rp == CLAW2_RP_EULER_4WAVE || p->rp == CLAW2_RP_EULER_5WAVE || p->rp == CLAW2_RP_SHALLOW_ROE);
+}
+
 void tiles(const claw2_problem* p, int* nbx, int* nby)
 {
     const bool split = p->transverse < 0;
@@ -418,12 +430,25 @@ void tiles(const claw2_problem* p, int* nbx, int* nby)
                        (p->rp == CLAW2_RP_ACOUSTICS || p->rp == CLAW2_RP_VC_ACOUSTICS);
     if (light && light_small_grid(p->mx, p->my)) tx = ty = LIGHT_SMALL_TILE;
     // the lean body's tiles (launch_step_t)
-    const bool lean = !split && p->index_capa < 0 && !p->use_fwave &&
-                      (p->rp == CLAW2_RP_EULER_4WAVE || p->rp == CLAW2_RP_EULER_5WAVE ||
-                       p->rp == CLAW2_RP_SHALLOW_ROE);
-    if (lean) { tx = LTX; ty = LTY; }
+    if (lean_body(p)) { tx = LTX; ty = LTY; }
     *nbx = (p->mx + tx - 1) / tx;
     *nby = (p->my + ty - 1) / ty;
+}
+
+// The scratch of a step: the 64-byte header (the arrival counter) and one
+// CFL partial per tile.
+size_t scratch_bytes(const claw2_problem* p)
+{
+    int nbx, nby;
+    tiles(p, &nbx, &nby);
+    return 64 + sizeof(double) * (size_t)nbx * (size_t)nby;
+}
+
+// Point a's arrival counter and partials into scratch.
+void set_scratch(void* scratch, StepArgs& a)
+{
+    a.ticket = static_cast<unsigned int*>(scratch);
+    a.partials = reinterpret_cast<double*>(static_cast<char*>(scratch) + 64);
 }
 
 void fill_args(const claw2_problem* p, double* q, StepArgs& a)
@@ -504,21 +529,28 @@ int halo_tensor_map(CUtensorMap* m, const double* q, const StepArgs& a, int meqn
 // bytes of halo that lean-body CTAs wait for in vain (claw2_debug_halo_shortfall)
 std::atomic<int> g_halo_shortfall{0};
 
-template <class RP>
-int launch_lean(const StepArgs& a0, int nbx, int nby, cudaStream_t st)
+template <class RP, int NT>
+int launch_lean_t(const StepArgs& a0, int nbx, int nby, cudaStream_t st)
 {
     StepArgs a = a0;
     a.halo_shortfall = g_halo_shortfall.load(std::memory_order_relaxed);
-    using SM = LeanSmem<RP, LTX, LTY, 256>;
-    auto kern = lean_step_kernel<RP>;
+    using SM = LeanSmem<RP, LTX, LTY, NT>;
+    auto kern = lean_step_kernel<RP, NT>;
     static std::atomic<uint64_t> optin{0};
     if (smem_optin(optin, kern, SM::bytes) != cudaSuccess) return CLAW2_ERR_CUDA;
     CUtensorMap tm0, tm1;
     int rc = halo_tensor_map(&tm0, a.ctrl ? a.q0 : a.qin, a, RP::MEQN);
     if (!rc) rc = a.ctrl ? halo_tensor_map(&tm1, a.q1, a, RP::MEQN) : (tm1 = tm0, CLAW2_OK);
     if (rc) return rc;
-    kern<<<dim3(nbx, nby), 256, SM::bytes, st>>>(a, tm0, tm1);
+    kern<<<dim3(nbx, nby), NT, SM::bytes, st>>>(a, tm0, tm1);
     return cudaGetLastError() == cudaSuccess ? CLAW2_OK : CLAW2_ERR_CUDA;
+}
+
+template <class RP>
+int launch_lean(const StepArgs& a, int nbx, int nby, cudaStream_t st)
+{
+    if ((long long)nbx * nby <= LEAN_BIG_BLOCK_TILES) return launch_lean_t<RP, 512>(a, nbx, nby, st);
+    return launch_lean_t<RP, 256>(a, nbx, nby, st);
 }
 
 template <class RP, bool SPLIT>
@@ -675,9 +707,7 @@ int claw2_get_layout(const claw2_problem* p, claw2_layout* out)
 size_t claw2_scratch_bytes(const claw2_problem* p)
 {
     if (!p || p->mx < 1 || p->my < 1) return 0;
-    int nbx, nby;
-    tiles(p, &nbx, &nby);
-    return 64 + sizeof(double) * (size_t)nbx * (size_t)nby;
+    return scratch_bytes(p);
 }
 
 int claw2_fill_ghosts(const claw2_problem* p, double* q, void* stream)
@@ -704,8 +734,7 @@ int claw2_step(const claw2_problem* p, const double* q_in, double* q_out, const 
     StepArgs a;
     fill_args(p, q_out, a);
     a.qin = q_in; a.qout = q_out; a.aux = aux; a.dt = dt;
-    a.ticket = static_cast<unsigned int*>(scratch);
-    a.partials = reinterpret_cast<double*>(static_cast<char*>(scratch) + 64);
+    set_scratch(scratch, a);
     a.cfl_out = cfl_dev;
     if ((rc = launch_step(p, a, S(stream)))) return rc;
     if (!a.ghost_fused)
@@ -722,8 +751,7 @@ int claw2_advance(const claw2_problem* p, double* q0, double* q1, const double* 
     StepArgs a;
     fill_args(p, q0, a);
     a.q0 = q0; a.q1 = q1; a.aux = aux; a.ctrl = ctrl;
-    a.ticket = static_cast<unsigned int*>(scratch);
-    a.partials = reinterpret_cast<double*>(static_cast<char*>(scratch) + 64);
+    set_scratch(scratch, a);
     for (int n = 0; n < nsteps; n++) {
         if ((rc = launch_step(p, a, S(stream)))) return rc;
         if (!a.ghost_fused &&
@@ -780,8 +808,7 @@ int claw2_advance_hooked(const claw2_problem* p, double* q0, double* q1, const d
     StepArgs a;
     fill_args(p, q0, a);
     a.q0 = q0; a.q1 = q1; a.aux = aux; a.ctrl = ctrl;
-    a.ticket = static_cast<unsigned int*>(scratch);
-    a.partials = reinterpret_cast<double*>(static_cast<char*>(scratch) + 64);
+    set_scratch(scratch, a);
     if ((rc = apply_hooks(p, hooks, a))) return rc;
     for (int n = 0; n < nsteps; n++) {
         if ((rc = launch_aux_from_q(hooks, a, const_cast<double*>(aux), q0, q1, ctrl, S(stream)))) return rc;
@@ -803,8 +830,7 @@ int claw2_advance_gauged(const claw2_problem* p, double* q0, double* q1, const d
     StepArgs a;
     fill_args(p, q0, a);
     a.q0 = q0; a.q1 = q1; a.aux = aux; a.ctrl = ctrl;
-    a.ticket = static_cast<unsigned int*>(scratch);
-    a.partials = reinterpret_cast<double*>(static_cast<char*>(scratch) + 64);
+    set_scratch(scratch, a);
     if (hooks && (rc = apply_hooks(p, hooks, a))) return rc;
     const int threads = 128;
     for (int n = 0; n < nsteps; n++) {
@@ -831,8 +857,7 @@ int claw2_step_ctrl(const claw2_problem* p, double* q0, double* q1, const double
     a.ctrl_readonly = 1;
     a.cfl_out = cfl_dev;
     a.ghost_fused = 0;
-    a.ticket = static_cast<unsigned int*>(scratch);
-    a.partials = reinterpret_cast<double*>(static_cast<char*>(scratch) + 64);
+    set_scratch(scratch, a);
     return launch_step(p, a, S(stream));
 }
 

@@ -282,6 +282,98 @@ CLAW2_HD void lean_chunk(const StepArgs& a, Ctx& ctx, const double* H, double* Q
     }
 }
 
+// The CFL number of a tile whose whole input halo holds the one state q.
+// Every interface of both sweeps then joins two equal states: rpn2a returns
+// zero strengths and fluctuations and the speeds of q's Roe average with
+// itself, which are the same for every interface of a direction, so the
+// lanes' running maxima of dtn*s and -dtn*s are those of one solve per
+// direction.  `finite` is cleared when a speed is not finite (the full tile
+// step then runs, with its own handling of a non-physical state).  Not
+// inlined: the two solves it holds run once per tile and stay out of the
+// body's instruction stream.
+template <class RP>
+__device__ __noinline__ double lean_uniform_cfl(const double (&q)[RP::MEQN], const double* prm, double dtdx,
+                                                double dtdy, bool& finite)
+{
+    constexpr int MEQN = RP::MEQN, MW = RP::MW, NROE = RP::NROE;
+    double cflm = 0.0;
+    auto direction = [&](auto D, double dtn) {
+        constexpr int IXY = decltype(D)::value;
+        double alpha[MW], amdq[MEQN], apdq[MEQN], roe[NROE];
+#pragma unroll
+        for (int p = 0; p < MW; p++) alpha[p] = 0.0;
+#pragma unroll
+        for (int r = 0; r < NROE; r++) roe[r] = 0.0;
+        const typename RP::Cell L = RP::template cell<IXY>(q, prm);
+        RP::template rpn2a<IXY>(q, q, L, L, prm, alpha, amdq, apdq, roe);
+        static_for<MW>([&](auto P) {
+            const double sp = RP::template speed<decltype(P)::value>(roe);
+            finite = finite && isfinite(sp);
+            const double c1 = dtn * sp, c2 = -dtn * sp;
+            cflm = cflm > c1 ? cflm : c1;
+            cflm = cflm > c2 ? cflm : c2;
+        });
+    };
+    direction(IntC<1>{}, dtdx);
+    direction(IntC<2>{}, dtdy);
+    return cflm;
+}
+
+// True in every thread when the tile's input halo (rows j0-2..j0+TY+1,
+// columns i0-2..i0+TX+1, clipped to the ghosted array: every cell either sweep
+// reads) holds one state.  A NaN never compares equal, so a non-finite halo
+// is never uniform.
+template <class RP, int TX, int TY, int TR>
+__device__ __forceinline__ bool lean_uniform_halo(const StepArgs& a, const double* H, int i0, int j0, int tid, int nt)
+{
+    constexpr int MEQN = RP::MEQN;
+    const int rmax = a.my + 3 - j0, cmax = a.mx + 3 - i0;   // last halo row / column inside the array
+    bool same = true;
+    for (int e = tid; e < TR * 32; e += nt) {
+        const int r = e >> 5, c = e & 31;
+        if (r <= rmax && c <= cmax) {
+#pragma unroll
+            for (int m = 0; m < MEQN; m++)
+                same = same && H[lean_hidx<MEQN, TR>(m, r, c)] == H[lean_hidx<MEQN, TR>(m, 0, 0)];
+        }
+    }
+    return __syncthreads_and(same);
+}
+
+// The two sweeps of the full tile step over the staged halo H; returns this
+// thread's running CFL maximum.
+template <class RP, int TX, int TY, int NT, class Ctx>
+__device__ __forceinline__ double lean_tile_sweeps(const StepArgs& a, Ctx& ctx, const double* H, double* Qx, double* CX,
+                                                   int i0, int j0, double dtdx, double dtdy)
+{
+    constexpr int MEQN = RP::MEQN;
+    constexpr int LPC = NT / 32;
+    const int warp = ctx.tid() >> 5;
+    double cflm = 0.0;
+    int chunk = 0;
+    {
+        const int first = j0 - 1;
+        const int last = (j0 + TY < a.my) ? j0 + TY : a.my;
+        for (int c0 = first; c0 <= last; c0 += LPC, chunk++) {
+            const int line = c0 + warp;
+            const int clast = (c0 + LPC - 1 < last) ? c0 + LPC - 1 : last;
+            lean_chunk<RP, 1, TX, TY, NT>(a, ctx, H, Qx, CX + (chunk & 1) * 2 * MEQN * NT, i0, j0, line, c0, clast,
+                                          line <= last, dtdx, dtdy, cflm);
+        }
+    }
+    {
+        const int first = i0 - 1;
+        const int last = (i0 + TX < a.mx) ? i0 + TX : a.mx;
+        for (int c0 = first; c0 <= last; c0 += LPC, chunk++) {
+            const int line = c0 + warp;
+            const int clast = (c0 + LPC - 1 < last) ? c0 + LPC - 1 : last;
+            lean_chunk<RP, 2, TX, TY, NT>(a, ctx, H, Qx, CX + (chunk & 1) * 2 * MEQN * NT, i0, j0, line, c0, clast,
+                                          line <= last, dtdy, dtdx, cflm);
+        }
+    }
+    return cflm;
+}
+
 // Whole-tile unsplit step with the lean body (the caller checks that the
 // problem has no capacity function and no f-waves).  tm0 / tm1: tensor maps
 // of the input state (uncontrolled mode: both of a.qin; controlled mode: of
@@ -297,7 +389,6 @@ __device__ __forceinline__ void lean_tile_at(const StepArgs& a, Ctx& ctx, const 
 {
     constexpr int MEQN = RP::MEQN;
     using SM = LeanSmem<RP, TX, TY, NT>;
-    constexpr int LPC = NT / 32;
     static_assert(TX + 4 <= 32 && TY + 4 <= 32, "a line's cells i0-2 .. i0+TX+1 must fit its 32 lanes");
     static_assert(RP::MAUX == 0, "the lean body serves the solvers without aux arrays");
     double* H = ctx.smem();
@@ -309,7 +400,6 @@ __device__ __forceinline__ void lean_tile_at(const StepArgs& a, Ctx& ctx, const 
     double* CX = Qx + SM::QX;
     double* red = CX + SM::CX;
     const int tid = ctx.tid();
-    const int warp = tid >> 5;
     const int i0 = tile.bx * TX, j0 = tile.by * TY;
     double* qout = a.qout;
     double dt = a.dt;
@@ -331,36 +421,33 @@ __device__ __forceinline__ void lean_tile_at(const StepArgs& a, Ctx& ctx, const 
     }
     const double dtdx = dt / a.dx, dtdy = dt / a.dy;
     double cflm = 0.0;
-    int chunk = 0;
     ctx.sync();                                    // the barrier is initialised
-    const bool late = !mbar_wait_bounded(bar, 0, kTmaWaitCycles);
-    if (__syncthreads_or(late)) {                  // the whole CTA takes the same path
+    // the whole CTA takes the same path
+    const bool fault = __syncthreads_or(!mbar_wait_bounded(bar, 0, kTmaWaitCycles));
+    bool keep = false;                             // the tile's cells keep their values
+    if (fault) {
         mbar_wait_bounded(bar, 0, kTmaWaitCycles);  // let a late copy land before the CTA moves on
-        finish_tile<MEQN, TX, TY, NT, SM::QP>(a, ctx, tile, Qx, TY * SM::QP, red, qout, i0, j0, 0.0, dt, true);
-        return;
-    }
-    {
-        const int first = j0 - 1;
-        const int last = (j0 + TY < a.my) ? j0 + TY : a.my;
-        for (int c0 = first; c0 <= last; c0 += LPC, chunk++) {
-            const int line = c0 + warp;
-            const int clast = (c0 + LPC - 1 < last) ? c0 + LPC - 1 : last;
-            lean_chunk<RP, 1, TX, TY, NT>(a, ctx, H, Qx, CX + (chunk & 1) * 2 * MEQN * NT, i0, j0, line, c0, clast,
-                                          line <= last, dtdx, dtdy, cflm);
+    } else if (lean_uniform_halo<RP, TX, TY, SM::TR>(a, H, i0, j0, tid, NT)) {
+        // A tile whose input halo holds one state has zero waves and
+        // fluctuations at every interface: its cells keep their values (the
+        // full step adds only zeros) and only its CFL number is computed.
+        double q0[MEQN];
+#pragma unroll
+        for (int m = 0; m < MEQN; m++) q0[m] = H[lean_hidx<MEQN, SM::TR>(m, 0, 0)];
+        bool finite = true;
+        const double cu = lean_uniform_cfl<RP>(q0, a.prm, dtdx, dtdy, finite);
+        if (finite) {                              // the same in every thread
+            for (int e = tid; e < TY * SM::QP; e += NT) {
+#pragma unroll
+                for (int m = 0; m < MEQN; m++) Qx[m * TY * SM::QP + e] = q0[m];
+            }
+            cflm = cu;
+            keep = true;
         }
     }
-    {
-        const int first = i0 - 1;
-        const int last = (i0 + TX < a.mx) ? i0 + TX : a.mx;
-        for (int c0 = first; c0 <= last; c0 += LPC, chunk++) {
-            const int line = c0 + warp;
-            const int clast = (c0 + LPC - 1 < last) ? c0 + LPC - 1 : last;
-            lean_chunk<RP, 2, TX, TY, NT>(a, ctx, H, Qx, CX + (chunk & 1) * 2 * MEQN * NT, i0, j0, line, c0, clast,
-                                          line <= last, dtdy, dtdx, cflm);
-        }
-    }
+    if (!fault && !keep) cflm = lean_tile_sweeps<RP, TX, TY, NT>(a, ctx, H, Qx, CX, i0, j0, dtdx, dtdy);
     ctx.sync();
-    finish_tile<MEQN, TX, TY, NT, SM::QP>(a, ctx, tile, Qx, TY * SM::QP, red, qout, i0, j0, cflm, dt);
+    finish_tile<MEQN, TX, TY, NT, SM::QP>(a, ctx, tile, Qx, TY * SM::QP, red, qout, i0, j0, cflm, dt, fault);
 }
 
 }  // namespace claw2

@@ -45,11 +45,14 @@ def test_validate_and_layout():
     L = _lib.layout(p)
     assert L.ld % 16 == 0 and L.ld >= 1284 and L.rows == 324
     assert L.plane == L.ld * L.rows and L.q_elems == 4 * L.plane
-    # one double per CTA: the unsplit Euler step runs 28 x 28 tiles (lean
-    # body), the split step 28 x 28, the acoustics bodies 29 x 29 (13 x 13 on
-    # grids of fewer than 148 such tiles)
+    # a 64-byte header and one double per CTA: the unsplit Euler step runs
+    # 28 x 28 tiles (lean body), the split step 28 x 28, the acoustics bodies
+    # 29 x 29 (13 x 13 on grids of fewer than 148 such tiles)
     nb = lib.claw2_scratch_bytes(ctypes.byref(p))
-    assert nb == 64 + 8 * ((1280 + 27) // 28) * ((320 + 27) // 28)
+    nt = ((1280 + 27) // 28) * ((320 + 27) // 28)
+    assert nb == 64 + 8 * nt
+    ps = H.problem("euler4", 1280, 320, -1)
+    assert lib.claw2_scratch_bytes(ctypes.byref(ps)) == 64 + 8 * nt
     pa = H.problem("acoustics", 1280, 320, 2)
     assert lib.claw2_scratch_bytes(ctypes.byref(pa)) == 64 + 8 * ((1280 + 28) // 29) * ((320 + 28) // 29)
     pa = H.problem("acoustics", 256, 256, 2)

@@ -223,3 +223,97 @@ def test_halo_wait_runs_out_and_reports_timeout(orc):
     ref = orc.Run(p, q, None, cfl_max=1.0, cfl_desired=0.9, dt_initial=0.002)
     ref.evolve_to_time(0.01)
     assert np.array_equal(got, ref.q) and ref.steps_taken == out.numsteps
+
+
+def _piecewise_uniform(p, kind, seed):
+    """Fields made of uniform regions: a background state, a second uniform
+    state over x >= 0.6 (its edge is a straight discontinuity), a noisy patch,
+    and for kind 'still' a zero-velocity background (wall ghosts then mirror
+    it exactly)."""
+    rng = np.random.default_rng(seed)
+    mx, my = p.mx, p.my
+    x = (np.arange(mx) + 0.5) / mx
+    y = (np.arange(my) + 0.5) / my
+    X, Y = np.meshgrid(x, y, indexing='ij')
+    right = X >= 0.6
+    patch = (np.abs(X - 0.25) < 0.12) & (np.abs(Y - 0.4) < 0.15)
+    noise = rng.random((mx, my))
+    q = np.empty((p.num_eqn, mx, my), order='F')
+    u0, v0 = (0.0, 0.0) if kind == "still" else (0.3, -0.2)
+    if p.rp in (_abi.RP_EULER_4WAVE, _abi.RP_EULER_5WAVE):
+        rho = np.where(right, 0.5, 1.0) + patch * 0.3 * noise
+        u = np.where(right, u0 - 0.1, u0) + patch * 0.1 * noise
+        v = np.full((mx, my), v0)
+        pr = np.where(right, 0.7, 1.0) + patch * 0.2 * noise
+        q[0] = rho
+        q[1] = rho * u
+        q[2] = rho * v
+        q[3] = pr / 0.4 + 0.5 * rho * (u * u + v * v)
+        if p.num_eqn == 5:
+            q[4] = right * 1.0
+    else:
+        h = np.where(right, 1.5, 1.0) + patch * 0.2 * noise
+        q[0] = h
+        q[1] = h * (u0 + patch * 0.1 * noise)
+        q[2] = h * v0
+    return q
+
+
+from pyclaw_b200 import _abi  # noqa: E402
+
+UNIFORM_CASES = [
+    ("euler4", 2, (1, 1), (1, 1), "moving", 150, 90),
+    ("euler4", 1, (1, 3), (3, 1), "moving", 150, 90),
+    ("euler4", 0, (3, 3), (3, 3), "still", 150, 90),
+    ("euler4", 2, (3, 3), (3, 3), "still", 57, 85),      # partial tiles on both axes
+    ("euler4", 2, (2, 1), (2, 1), "moving", 112, 56),    # periodic x: 4 x 2 full tiles
+    ("euler5", 2, (1, 3), (1, 3), "moving", 150, 90),
+    ("shallow", 2, (1, 1), (1, 1), "moving", 150, 90),
+    ("shallow", 2, (3, 3), (3, 3), "still", 130, 70),
+    ("shallow", 1, (1, 2), (1, 2), "moving", 100, 100),
+    # more than 8 x 148 tiles: the lean body's 256-thread form (the grids
+    # above run its 512-thread form)
+    ("euler4", 2, (1, 3), (3, 1), "moving", 1000, 980),
+    ("shallow", 2, (3, 3), (3, 3), "still", 1010, 1000),
+]
+
+
+@pytest.mark.parametrize("name,tr,bcl,bcu,kind,mx,my", UNIFORM_CASES)
+def test_uniform_tiles_bit_identical_to_oracle(orc, name, tr, bcl, bcu, kind, mx, my):
+    """Tiles whose whole input halo holds one state take the lean body's short
+    path (cells kept, CFL from one solve per direction); next to them tiles
+    that straddle a discontinuity or the noisy patch take the full step.
+    Three steps in a row, each compared with the oracle (values, CFL, ghost
+    cells), so tiles change kind as the disturbance spreads."""
+    p = H.problem(name, mx, my, tr, bcl=bcl, bcu=bcu)
+    q = _piecewise_uniform(p, kind, seed=mx + my + tr)
+    qbc = orc.new_qbc(p, q)
+    orc.fill_ghosts(p, qbc)
+    dt = 0.2 / max(mx, my)
+    for _ in range(3):
+        ref = qbc.copy(order="F")
+        cfl_ref = orc.step_hyperbolic(p, ref, None, dt)
+        out, cfl = H.dev_step(p, qbc, None, dt)
+        assert np.array_equal(out[I], ref[I]), np.nanmax(np.abs(out[I] - ref[I]))
+        assert cfl == cfl_ref, (cfl, cfl_ref)
+        orc.fill_ghosts(p, ref)
+        assert np.array_equal(out, ref), "ghost cells differ from the boundary fill of the new state"
+        qbc = np.asfortranarray(ref)
+
+
+@pytest.mark.parametrize("name", ["euler4", "shallow"])
+def test_all_uniform_grid_keeps_its_state_and_cfl(orc, name):
+    """A grid holding one state everywhere: every tile takes the short path;
+    the state is unchanged and the CFL number equals the oracle's."""
+    p = H.problem(name, 97, 61, 2, bcl=(1, 1), bcu=(1, 1))
+    q = _piecewise_uniform(p, "moving", seed=1)
+    q[:] = q[:, :1, :1]
+    qbc = orc.new_qbc(p, q)
+    orc.fill_ghosts(p, qbc)
+    dt = 0.3 / 97
+    ref = qbc.copy(order="F")
+    cfl_ref = orc.step_hyperbolic(p, ref, None, dt)
+    out, cfl = H.dev_step(p, qbc, None, dt)
+    assert np.array_equal(out, ref) and np.array_equal(out[I], qbc[I])
+    assert cfl == cfl_ref and cfl > 0.0
+
