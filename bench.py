@@ -464,6 +464,9 @@ def run_ours(args, world, rank, local):
     dev.ctrl_host.copy_(dev.ctrl)
     torch.cuda.synchronize()
     t_timed0 = host.t
+    dt_timed0 = host.dt
+    # the e2e legs start from the same developed state (one grid: rank 0's)
+    q_timed0 = dev.download_q() if world == 1 else q
 
     for _ in range(max(3, args.warmup)):
         flush.fill_(1.0)
@@ -525,8 +528,9 @@ def run_ours(args, world, rank, local):
     # ---- e2e through the host-buffer C ABI (claw2_session_evolve) ----------
     e2e = e2e_s2 = None
     if rank == 0 or world > 1:
-        e2e = _e2e(lib, prob, q, run, args)
-        e2e_s2 = _e2e_step2(lib, prob, q, run, args)
+        t_e, dt_e = (t_timed0, dt_timed0) if world == 1 else (0.0, None)
+        e2e = _e2e(lib, prob, q_timed0, run, args, t_e, dt_e)
+        e2e_s2 = _e2e_step2(lib, prob, q_timed0, run, args, dt_e)
     e2e_val = _sum_over_ranks(e2e["value"], world) if e2e else None
     e2e_s2_val = _sum_over_ranks(e2e_s2["value"], world) if e2e_s2 else None
 
@@ -573,6 +577,8 @@ def run_ours(args, world, rank, local):
                     "steps_per_call": e2e["steps"], "calls": e2e["calls"],
                     "api": "claw2_session_evolve (one Controller.run output interval per call; the steps of a "
                            "call run back to back, L2 not flushed)",
+                    "start": "the developed state of the timed steps (t = %.4f), uploaded from pinned host memory"
+                             % t_timed0 if world == 1 else "t = 0",
                     "per_step_f2py_contract": {
                         "value": e2e_s2_val, "unit": "cell-updates/s", "api": "claw2_session_step2",
                         "h2d_bytes_per_step": e2e_s2["h2d"], "d2h_bytes_per_step": e2e_s2["d2h"],
@@ -596,10 +602,11 @@ def run_ours(args, world, rank, local):
         print(json.dumps(line), flush=True)
 
 
-def _e2e(lib, prob, q, run, args):
+def _e2e(lib, prob, q, run, args, t_start=0.0, dt_start=None):
     """claw2_session_evolve from pinned host buffers: each call uploads the
     state, advances it by a fixed simulated interval with on-device dt
-    control, and downloads it again."""
+    control, and downloads it again.  q is the state at t_start (dt_start:
+    the controller's dt there)."""
     import torch
     s = ctypes.c_void_p()
     from pyclaw_b200 import _lib
@@ -607,8 +614,8 @@ def _e2e(lib, prob, q, run, args):
     try:
         host = torch.from_numpy(np.asfortranarray(q).ravel(order='K')).clone().pin_memory()
         hq = host.numpy()
-        t = ctypes.c_double(0.0)
-        dt = ctypes.c_double(run['dt_initial'])
+        t = ctypes.c_double(t_start)
+        dt = ctypes.c_double(dt_start if dt_start else run['dt_initial'])
         status = (ctypes.c_double * 5)()
         interval = 40 * run['dt_initial']
         def call():
@@ -657,7 +664,7 @@ def _ghosted(prob, q):
     return qbc
 
 
-def _e2e_step2(lib, prob, q, run, args):
+def _e2e_step2(lib, prob, q, run, args, dt_step=None):
     """claw2_session_step2, the per-step f2py contract of step2: every call
     copies the ghosted state in the reference's layout from pinned host
     memory, converts it, takes one step, converts back and copies the result
@@ -671,7 +678,7 @@ def _e2e_step2(lib, prob, q, run, args):
         bufs = [torch.from_numpy(qbc.ravel(order='F')).clone().pin_memory() for _ in range(2)]
         arrs = [b.numpy() for b in bufs]
         cfl = ctypes.c_double()
-        dt = run['dt_initial']
+        dt = dt_step if dt_step else run['dt_initial']
 
         def call(k):
             return lib.claw2_session_step2(s, arrs[k & 1].ctypes.data, arrs[(k + 1) & 1].ctypes.data, None, dt,
