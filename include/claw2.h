@@ -359,7 +359,10 @@ typedef struct claw2_batch_instance {
     int32_t pad_;
 } claw2_batch_instance;
 
-/* Launch configurations of the batched kernel the autotuner chooses from. */
+/* Launch configurations of the batched kernel the autotuner chooses from:
+ * threads per CTA x resident CTAs per SM x tile edge, and the grid's form
+ * (variants 0-9: a persistent grid of SMs x resident CTAs, each CTA walking a
+ * contiguous run of tiles; 10-13: one CTA per tile). */
 CLAW2_EXPORT int claw2_batch_num_variants(void);
 /* Threads per CTA and resident CTAs per SM of variant v (for reporting). */
 CLAW2_EXPORT int claw2_batch_variant_info(int v, int* threads, int* ctas_per_sm);

@@ -202,6 +202,32 @@ batch_kernel(const claw2_batch_instance* __restrict__ inst, int ninst, int ntile
     }
 }
 
+// Batched step with one CTA per tile (grid = all tiles of all instances):
+// the hardware hands tiles to SMs as slots free up, so uneven tiles balance
+// themselves, and no loop state stays live across the tile body.  The tile's
+// instance comes from a binary search over the descriptors (their first
+// levels stay in L1 and L2 across CTAs); there is no L2 prefetch of a next
+// tile, the other resident CTAs cover the first loads.
+template <class RP, int NT, int MINB, bool LIGHT, int T>
+__global__ void __launch_bounds__(NT, MINB)
+batch_tile_kernel(const claw2_batch_instance* __restrict__ inst, int ninst, StepArgs common)
+{
+    static_assert(LIGHT || T == 29, "the generic body runs 29x29 tiles in the batch");
+    extern __shared__ double smem_dyn[];
+    DevCtx ctx{smem_dyn};
+    const int t = (int)blockIdx.x;
+    const claw2_batch_instance& I = inst[batch_instance_of(inst, ninst, t)];
+    StepArgs a = common;
+    a.q0 = I.q0; a.q1 = I.q1; a.aux = I.aux; a.ctrl = I.ctrl;
+    a.partials = I.partials; a.ticket = I.ticket;
+    a.ld = I.ld; a.plane = I.plane; a.mx = I.mx; a.my = I.my; a.dx = I.dx; a.dy = I.dy;
+    a.ghost_fused = (I.mx >= 4 && I.my >= 4) ? common.ghost_fused : 0;
+    const int lt = t - I.tile_begin;
+    const TileId tile{lt % I.nbx, lt / I.nbx, I.nbx, I.nby, lt, I.nbx * I.nby};
+    if constexpr (LIGHT) light_tile_at<RP, T, T, NT>(a, ctx, tile);
+    else step_tile_at<RP, 29, 29, NT, false>(a, ctx, tile);
+}
+
 // Tile shapes: a line of a chunk has 32 interface slots, so TX+3, TY+3 <= 32.
 #ifndef CLAW2_UNT
 #define CLAW2_UNT 256
@@ -953,10 +979,13 @@ namespace {
 // (claw2_batch_advance returns CLAW2_ERR_UNSUPPORTED for them with the other
 // solvers); a line of the light body has 32 lanes for tile + 3 interfaces, so
 // smaller tiles leave lanes idle but waste fewer cells at instance edges.
-struct BatchVariant { int threads, minb, tile; };
-constexpr BatchVariant kBatchVariants[] = {{256, 2, 29}, {128, 4, 29}, {128, 3, 29}, {512, 1, 29},
-                                           {256, 3, 29}, {256, 4, 29}, {256, 3, 21}, {256, 4, 21},
-                                           {256, 3, 13}, {256, 4, 13}};
+// persistent: a grid of SMs x resident CTAs walking contiguous runs of tiles
+// (batch_kernel); otherwise one CTA per tile (batch_tile_kernel)
+struct BatchVariant { int threads, minb, tile, persistent; };
+constexpr BatchVariant kBatchVariants[] = {{256, 2, 29, 1}, {128, 4, 29, 1}, {128, 3, 29, 1}, {512, 1, 29, 1},
+                                           {256, 3, 29, 1}, {256, 4, 29, 1}, {256, 3, 21, 1}, {256, 4, 21, 1},
+                                           {256, 3, 13, 1}, {256, 4, 13, 1}, {256, 3, 29, 0}, {256, 4, 29, 0},
+                                           {128, 6, 29, 0}, {512, 2, 29, 0}};
 constexpr int kNumBatchVariants = sizeof(kBatchVariants) / sizeof(kBatchVariants[0]);
 
 bool batch_tile_ok(int tile) { return tile == 29 || tile == 21 || tile == 13; }
@@ -989,6 +1018,21 @@ int batch_launch_t(const StepArgs& common, const claw2_batch_instance* inst, int
     return CLAW2_OK;
 }
 
+template <class RP, int NT, int MINB, bool LIGHT, int T>
+int batch_launch_tiles(const StepArgs& common, const claw2_batch_instance* inst, int ninst, int ntiles, int nsteps,
+                       cudaStream_t st)
+{
+    constexpr int SMB = LIGHT ? LightSmem<T, T, NT>::bytes : TileSmem<RP, 29, 29, NT, false>::bytes;
+    auto kern = batch_tile_kernel<RP, NT, MINB, LIGHT, T>;
+    static std::atomic<uint64_t> optin{0};
+    if (smem_optin(optin, kern, SMB) != cudaSuccess) return CLAW2_ERR_CUDA;
+    for (int n = 0; n < nsteps; n++) {
+        kern<<<ntiles, NT, SMB, st>>>(inst, ninst, common);
+        if (cudaGetLastError() != cudaSuccess) return CLAW2_ERR_CUDA;
+    }
+    return CLAW2_OK;
+}
+
 template <class RP>
 int batch_launch_rp(int variant, const StepArgs& c, const claw2_batch_instance* inst, int ninst, int ntiles,
                     int nsteps, cudaStream_t st)
@@ -1006,6 +1050,10 @@ int batch_launch_rp(int variant, const StepArgs& c, const claw2_batch_instance* 
             case 7: return batch_launch_t<RP, 256, 4, true, 21>(c, inst, ninst, ntiles, nsteps, st);
             case 8: return batch_launch_t<RP, 256, 3, true, 13>(c, inst, ninst, ntiles, nsteps, st);
             case 9: return batch_launch_t<RP, 256, 4, true, 13>(c, inst, ninst, ntiles, nsteps, st);
+            case 10: return batch_launch_tiles<RP, 256, 3, true, 29>(c, inst, ninst, ntiles, nsteps, st);
+            case 11: return batch_launch_tiles<RP, 256, 4, true, 29>(c, inst, ninst, ntiles, nsteps, st);
+            case 12: return batch_launch_tiles<RP, 128, 6, true, 29>(c, inst, ninst, ntiles, nsteps, st);
+            case 13: return batch_launch_tiles<RP, 512, 2, true, 29>(c, inst, ninst, ntiles, nsteps, st);
             default: return CLAW2_ERR_INVALID;
             }
         }
