@@ -90,6 +90,13 @@ lean_step_kernel(StepArgs a, const __grid_constant__ CUtensorMap tm0, const __gr
 {
     extern __shared__ double smem_dyn[];
     __shared__ __align__(8) uint64_t halo_bar;
+    // Chained steps (launch_lean_t with chained set): once every CTA of this
+    // step has started, the next step's CTAs may start on the SMs this step
+    // frees and wait here until this step has completed and its writes are
+    // visible.  Launched without the attribute both instructions return at
+    // once.
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    asm volatile("griddepcontrol.wait;" ::: "memory");
     DevCtx ctx{smem_dyn};
     const TileId t{(int)blockIdx.x, (int)blockIdx.y, (int)gridDim.x, (int)gridDim.y,
                    (int)(blockIdx.y * gridDim.x + blockIdx.x), (int)(gridDim.x * gridDim.y)};
@@ -555,8 +562,11 @@ int halo_tensor_map(CUtensorMap* m, const double* q, const StepArgs& a, int meqn
 // bytes of halo that lean-body CTAs wait for in vain (claw2_debug_halo_shortfall)
 std::atomic<int> g_halo_shortfall{0};
 
+// chained: the previous operation in the stream is a step kernel of the same
+// device loop, so this launch may overlap its end (programmatic dependent
+// launch; the kernel waits for it before reading anything).
 template <class RP, int NT>
-int launch_lean_t(const StepArgs& a0, int nbx, int nby, cudaStream_t st)
+int launch_lean_t(const StepArgs& a0, int nbx, int nby, cudaStream_t st, bool chained)
 {
     StepArgs a = a0;
     a.halo_shortfall = g_halo_shortfall.load(std::memory_order_relaxed);
@@ -568,24 +578,37 @@ int launch_lean_t(const StepArgs& a0, int nbx, int nby, cudaStream_t st)
     int rc = halo_tensor_map(&tm0, a.ctrl ? a.q0 : a.qin, a, RP::MEQN);
     if (!rc) rc = a.ctrl ? halo_tensor_map(&tm1, a.q1, a, RP::MEQN) : (tm1 = tm0, CLAW2_OK);
     if (rc) return rc;
-    kern<<<dim3(nbx, nby), NT, SM::bytes, st>>>(a, tm0, tm1);
-    return cudaGetLastError() == cudaSuccess ? CLAW2_OK : CLAW2_ERR_CUDA;
+    if (!chained) {
+        kern<<<dim3(nbx, nby), NT, SM::bytes, st>>>(a, tm0, tm1);
+        return cudaGetLastError() == cudaSuccess ? CLAW2_OK : CLAW2_ERR_CUDA;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(nbx, nby);
+    cfg.blockDim = dim3(NT);
+    cfg.dynamicSmemBytes = SM::bytes;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kern, a, tm0, tm1) == cudaSuccess ? CLAW2_OK : CLAW2_ERR_CUDA;
 }
 
 template <class RP>
-int launch_lean(const StepArgs& a, int nbx, int nby, cudaStream_t st)
+int launch_lean(const StepArgs& a, int nbx, int nby, cudaStream_t st, bool chained)
 {
-    if ((long long)nbx * nby <= LEAN_BIG_BLOCK_TILES) return launch_lean_t<RP, 512>(a, nbx, nby, st);
-    return launch_lean_t<RP, 256>(a, nbx, nby, st);
+    if ((long long)nbx * nby <= LEAN_BIG_BLOCK_TILES) return launch_lean_t<RP, 512>(a, nbx, nby, st, chained);
+    return launch_lean_t<RP, 256>(a, nbx, nby, st, chained);
 }
 
 template <class RP, bool SPLIT>
-int launch_step_t(const StepArgs& a, int nbx, int nby, cudaStream_t st)
+int launch_step_t(const StepArgs& a, int nbx, int nby, cudaStream_t st, bool chained)
 {
     if constexpr (!SPLIT && HasLight<RP>::value)
         if (a.capa < 0 && !a.fwave) return launch_light<RP>(a, nbx, nby, st);
     if constexpr (!SPLIT && HasLean<RP>::value)
-        if (a.capa < 0 && !a.fwave) return launch_lean<RP>(a, nbx, nby, st);
+        if (a.capa < 0 && !a.fwave) return launch_lean<RP>(a, nbx, nby, st, chained);
     constexpr int TX = SPLIT ? STX : UTX, TY = SPLIT ? STY : UTY, NT = SPLIT ? SNT : UNT;
     using SM = TileSmem<RP, TX, TY, NT, SPLIT>;
     auto kern = step_kernel<RP, TX, TY, NT, SPLIT>;
@@ -595,24 +618,25 @@ int launch_step_t(const StepArgs& a, int nbx, int nby, cudaStream_t st)
     return cudaGetLastError() == cudaSuccess ? CLAW2_OK : CLAW2_ERR_CUDA;
 }
 
-int launch_step(const claw2_problem* p, const StepArgs& a, cudaStream_t st)
+// chained: see launch_lean_t (only the lean body takes it up).
+int launch_step(const claw2_problem* p, const StepArgs& a, cudaStream_t st, bool chained = false)
 {
     int nbx, nby;
     tiles(p, &nbx, &nby);
     const bool split = p->transverse < 0;
     switch (p->rp) {
     case CLAW2_RP_ACOUSTICS:
-        return split ? launch_step_t<RpAcoustics, true>(a, nbx, nby, st) : launch_step_t<RpAcoustics, false>(a, nbx, nby, st);
+        return split ? launch_step_t<RpAcoustics, true>(a, nbx, nby, st, chained) : launch_step_t<RpAcoustics, false>(a, nbx, nby, st, chained);
     case CLAW2_RP_VC_ACOUSTICS:
-        return split ? launch_step_t<RpVcAcoustics, true>(a, nbx, nby, st) : launch_step_t<RpVcAcoustics, false>(a, nbx, nby, st);
+        return split ? launch_step_t<RpVcAcoustics, true>(a, nbx, nby, st, chained) : launch_step_t<RpVcAcoustics, false>(a, nbx, nby, st, chained);
     case CLAW2_RP_EULER_4WAVE:
-        return split ? launch_step_t<RpEuler<false>, true>(a, nbx, nby, st) : launch_step_t<RpEuler<false>, false>(a, nbx, nby, st);
+        return split ? launch_step_t<RpEuler<false>, true>(a, nbx, nby, st, chained) : launch_step_t<RpEuler<false>, false>(a, nbx, nby, st, chained);
     case CLAW2_RP_EULER_5WAVE:
-        return split ? launch_step_t<RpEuler<true>, true>(a, nbx, nby, st) : launch_step_t<RpEuler<true>, false>(a, nbx, nby, st);
+        return split ? launch_step_t<RpEuler<true>, true>(a, nbx, nby, st, chained) : launch_step_t<RpEuler<true>, false>(a, nbx, nby, st, chained);
     case CLAW2_RP_SHALLOW_ROE:
-        return split ? launch_step_t<RpShallow, true>(a, nbx, nby, st) : launch_step_t<RpShallow, false>(a, nbx, nby, st);
+        return split ? launch_step_t<RpShallow, true>(a, nbx, nby, st, chained) : launch_step_t<RpShallow, false>(a, nbx, nby, st, chained);
     case CLAW2_RP_PSYSTEM:
-        return split ? launch_step_t<RpPsystem, true>(a, nbx, nby, st) : launch_step_t<RpPsystem, false>(a, nbx, nby, st);
+        return split ? launch_step_t<RpPsystem, true>(a, nbx, nby, st, chained) : launch_step_t<RpPsystem, false>(a, nbx, nby, st, chained);
     default:
         return CLAW2_ERR_INVALID;
     }
@@ -779,7 +803,8 @@ int claw2_advance(const claw2_problem* p, double* q0, double* q1, const double* 
     a.q0 = q0; a.q1 = q1; a.aux = aux; a.ctrl = ctrl;
     set_scratch(scratch, a);
     for (int n = 0; n < nsteps; n++) {
-        if ((rc = launch_step(p, a, S(stream)))) return rc;
+        // from the second step on, a step follows a step kernel directly
+        if ((rc = launch_step(p, a, S(stream), n > 0 && a.ghost_fused))) return rc;
         if (!a.ghost_fused &&
             (rc = launch_fill(p, nullptr, p->num_eqn, p->bc_lower, p->bc_upper, false, q0, q1, ctrl, S(stream))))
             return rc;
