@@ -51,17 +51,6 @@ template <class RP, int TX, int TY, int NT> struct LeanSmem {
     static_assert((BOX * 8) % 1024 == 0, "each box starts on a 1024-byte boundary");
 };
 
-// f(IntC<0>{}), ..., f(IntC<N-1>{}): a loop whose index is a compile-time constant
-template <int N> struct IntC { static constexpr int value = N; };
-template <int N, int I = 0, class F>
-__device__ __forceinline__ void static_for(F&& f)
-{
-    if constexpr (I < N) {
-        f(IntC<I>{});
-        static_for<N, I + 1>(f);
-    }
-}
-
 // The staged input of halo row r, column c, field m: H holds q(m, i0-2+c, j0-2+r).
 template <int MEQN, int TR>
 __device__ __forceinline__ int lean_hidx(int m, int r, int c)
@@ -282,43 +271,6 @@ CLAW2_HD void lean_chunk(const StepArgs& a, Ctx& ctx, const double* H, double* Q
     }
 }
 
-// The CFL number of a tile whose whole input halo holds the one state q.
-// Every interface of both sweeps then joins two equal states: rpn2a returns
-// zero strengths and fluctuations and the speeds of q's Roe average with
-// itself, which are the same for every interface of a direction, so the
-// lanes' running maxima of dtn*s and -dtn*s are those of one solve per
-// direction.  `finite` is cleared when a speed is not finite (the full tile
-// step then runs, with its own handling of a non-physical state).  Not
-// inlined: the two solves it holds run once per tile and stay out of the
-// body's instruction stream.
-template <class RP>
-__device__ __noinline__ double lean_uniform_cfl(const double (&q)[RP::MEQN], const double* prm, double dtdx,
-                                                double dtdy, bool& finite)
-{
-    constexpr int MEQN = RP::MEQN, MW = RP::MW, NROE = RP::NROE;
-    double cflm = 0.0;
-    auto direction = [&](auto D, double dtn) {
-        constexpr int IXY = decltype(D)::value;
-        double alpha[MW], amdq[MEQN], apdq[MEQN], roe[NROE];
-#pragma unroll
-        for (int p = 0; p < MW; p++) alpha[p] = 0.0;
-#pragma unroll
-        for (int r = 0; r < NROE; r++) roe[r] = 0.0;
-        const typename RP::Cell L = RP::template cell<IXY>(q, prm);
-        RP::template rpn2a<IXY>(q, q, L, L, prm, alpha, amdq, apdq, roe);
-        static_for<MW>([&](auto P) {
-            const double sp = RP::template speed<decltype(P)::value>(roe);
-            finite = finite && isfinite(sp);
-            const double c1 = dtn * sp, c2 = -dtn * sp;
-            cflm = cflm > c1 ? cflm : c1;
-            cflm = cflm > c2 ? cflm : c2;
-        });
-    };
-    direction(IntC<1>{}, dtdx);
-    direction(IntC<2>{}, dtdy);
-    return cflm;
-}
-
 // True in every thread when the tile's input halo (rows j0-2..j0+TY+1,
 // columns i0-2..i0+TX+1, clipped to the ghosted array: every cell either sweep
 // reads) holds one state.  A NaN never compares equal, so a non-finite halo
@@ -435,7 +387,7 @@ __device__ __forceinline__ void lean_tile_at(const StepArgs& a, Ctx& ctx, const 
 #pragma unroll
         for (int m = 0; m < MEQN; m++) q0[m] = H[lean_hidx<MEQN, SM::TR>(m, 0, 0)];
         bool finite = true;
-        const double cu = lean_uniform_cfl<RP>(q0, a.prm, dtdx, dtdy, finite);
+        const double cu = uniform_cfl<RP>(q0, a.prm, dtdx, dtdy, finite);
         if (finite) {                              // the same in every thread
             for (int e = tid; e < TY * SM::QP; e += NT) {
 #pragma unroll

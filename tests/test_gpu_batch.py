@@ -95,3 +95,35 @@ def test_sharded_batch_shares_equal_the_whole_batch():
         sb.close()
     assert seen == set(range(len(insts)))
     whole.close()
+
+
+def test_batched_euler_one_state_tiles_equal_single_runs():
+    """Euler instances with regions of one state run the batch's generic
+    unsplit body; each must equal its solo run (the lean body, whose tiles of
+    one state keep their cells) bit for bit."""
+    rng = np.random.default_rng(4)
+    insts = []
+    for nx, ny in ((70, 45), (33, 90), (120, 64)):
+        x = (np.arange(nx) + 0.5) / nx
+        X = np.repeat(x[:, None], ny, axis=1)
+        rho = np.where(X < 0.5, 1.0, 0.6)
+        rho[:8, :8] += 0.2 * rng.random((8, 8))
+        q = np.empty((4, nx, ny), order="F")
+        q[0] = rho
+        q[1] = rho * 0.2
+        q[2] = 0.0
+        q[3] = 1.0 / 0.4 + 0.5 * rho * 0.04
+        insts.append(dict(q=q, aux=None, dx=1.0 / nx, dy=1.0 / ny, dt=0.2 / max(nx, ny)))
+    prob = _abi.make_problem(rp=_abi.RP_EULER_4WAVE, num_eqn=4, num_waves=4, num_aux=0, mx=64, my=64, dx=1.0,
+                             dy=1.0, order=2, transverse=2, mthlim=[4], params=(1.4, 0.4),
+                             bc_lower=(_abi.BC_EXTRAP, _abi.BC_WALL), bc_upper=(_abi.BC_EXTRAP, _abi.BC_WALL))
+    from pyclaw_b200.batch import BatchSolver
+    bs = BatchSolver(prob, insts)
+    bs.init_controls([i["dt"] for i in insts], max_steps=25)
+    bs.advance(25)
+    ctrls = bs.controls()
+    for k in range(len(insts)):
+        q_alone, c_alone = _alone(prob, insts[k], 25)
+        assert ctrls[k].numsteps == c_alone.numsteps and ctrls[k].t == c_alone.t and ctrls[k].dt == c_alone.dt
+        assert np.array_equal(bs.solution(k), q_alone)
+    bs.close()

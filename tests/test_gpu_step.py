@@ -275,6 +275,11 @@ UNIFORM_CASES = [
     # above run its 512-thread form)
     ("euler4", 2, (1, 3), (3, 1), "moving", 1000, 980),
     ("shallow", 2, (3, 3), (3, 3), "still", 1010, 1000),
+    # dimensional splitting: the generic body (28x28 tiles) on the same data
+    ("euler4", -1, (1, 3), (3, 1), "moving", 150, 90),
+    ("euler5", -1, (2, 1), (2, 1), "moving", 112, 56),
+    ("shallow", -1, (3, 3), (3, 3), "still", 130, 70),
+    ("shallow", -1, (1, 1), (1, 1), "moving", 57, 85),
 ]
 
 
@@ -317,3 +322,39 @@ def test_all_uniform_grid_keeps_its_state_and_cfl(orc, name):
     assert np.array_equal(out, ref) and np.array_equal(out[I], qbc[I])
     assert cfl == cfl_ref and cfl > 0.0
 
+
+
+@pytest.mark.parametrize("name,mx,my", [("euler4", 140, 84), ("shallow", 1010, 1000)])
+def test_chained_steps_equal_single_step_calls(name, mx, my):
+    """claw2_advance launches the lean body's steps after its first as
+    programmatic dependents of the step before; 30 steps in one call must
+    leave the state, t and dt bit for bit where 30 calls of one step do."""
+    import ctypes
+    from pyclaw_b200 import _abi, _lib
+    from pyclaw_b200.device import DeviceState
+    t = H.torch()
+    lib = _lib.load()
+    p = H.problem(name, mx, my, 2, bcl=(1, 3), bcu=(3, 1))
+    q = _piecewise_uniform(p, "moving", seed=9)
+    results = []
+    for calls in (1, 30):
+        dev = DeviceState(p)
+        dev.upload_q(q)
+        c = _abi.Control.from_address(dev.ctrl_host.data_ptr())
+        _lib.check(lib.claw2_control_init(ctypes.byref(c), 0.0, 0.2 / max(mx, my), 1e9, 1.0, 0.9, 1e99, 1, 0,
+                                          1 << 40, 0.9), "claw2_control_init")
+        dev.ctrl.copy_(dev.ctrl_host)
+        for _ in range(calls):
+            _lib.check(lib.claw2_advance(ctypes.byref(p), dev.ptr(dev.q[0]), dev.ptr(dev.q[1]), dev.ptr(dev.aux),
+                                         dev.ptr(dev.ctrl), dev.ptr(dev.scratch), 30 // calls, dev.stream),
+                       "claw2_advance")
+        t.cuda.synchronize()
+        dev.ctrl_host.copy_(dev.ctrl)
+        t.cuda.synchronize()
+        c = _abi.Control.from_address(dev.ctrl_host.data_ptr())
+        assert c.numsteps == 30 and c.error == 0
+        dev.cur = c.cur
+        results.append((dev.download_q(), c.t, c.dt))
+    (qa, ta, da), (qb, tb, db) = results
+    assert ta == tb and da == db
+    assert np.array_equal(qa, qb)
