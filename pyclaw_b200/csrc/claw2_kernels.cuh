@@ -709,35 +709,38 @@ __device__ __forceinline__ void static_for(F&& f)
 // zero strengths and fluctuations and the speeds of q's Roe average with
 // itself, which are the same for every interface of a direction, so the
 // lanes' running maxima of dtn*s and -dtn*s are those of one solve per
-// direction.  `finite` is cleared when a speed is not finite (the full tile
-// step then runs, with its own handling of a non-physical state).  Not
-// inlined: the two solves it holds run once per tile and stay out of the
-// body's instruction stream.
+// direction; the y solve's speeds follow from the x solve's Roe averages
+// (RP::speed_other).  `finite` is cleared when a speed is not finite (the
+// full tile step then runs, with its own handling of a non-physical state).
+// Not inlined: it runs once per tile and stays out of the body's
+// instruction stream.
 template <class RP>
 __device__ __noinline__ double uniform_cfl(const double (&q)[RP::MEQN], const double* prm, double dtdx, double dtdy,
                                            bool& finite)
 {
     constexpr int MEQN = RP::MEQN, MW = RP::MW, NROE = RP::NROE;
+    double alpha[MW], amdq[MEQN], apdq[MEQN], roe[NROE];
+#pragma unroll
+    for (int p = 0; p < MW; p++) alpha[p] = 0.0;
+#pragma unroll
+    for (int r = 0; r < NROE; r++) roe[r] = 0.0;
+    const typename RP::Cell L = RP::template cell<1>(q, prm);
+    RP::template rpn2a<1>(q, q, L, L, prm, alpha, amdq, apdq, roe);
     double cflm = 0.0;
-    auto direction = [&](auto D, double dtn) {
-        constexpr int IXY = decltype(D)::value;
-        double alpha[MW], amdq[MEQN], apdq[MEQN], roe[NROE];
-#pragma unroll
-        for (int p = 0; p < MW; p++) alpha[p] = 0.0;
-#pragma unroll
-        for (int r = 0; r < NROE; r++) roe[r] = 0.0;
-        const typename RP::Cell L = RP::template cell<IXY>(q, prm);
-        RP::template rpn2a<IXY>(q, q, L, L, prm, alpha, amdq, apdq, roe);
-        static_for<MW>([&](auto P) {
-            const double sp = RP::template speed<decltype(P)::value>(roe);
-            finite = finite && isfinite(sp);
-            const double c1 = dtn * sp, c2 = -dtn * sp;
-            cflm = cflm > c1 ? cflm : c1;
-            cflm = cflm > c2 ? cflm : c2;
-        });
-    };
-    direction(IntC<1>{}, dtdx);
-    direction(IntC<2>{}, dtdy);
+    static_for<MW>([&](auto P) {
+        const double sp = RP::template speed<decltype(P)::value>(roe);
+        finite = finite && isfinite(sp);
+        const double c1 = dtdx * sp, c2 = -dtdx * sp;
+        cflm = cflm > c1 ? cflm : c1;
+        cflm = cflm > c2 ? cflm : c2;
+    });
+    static_for<MW>([&](auto P) {
+        const double sp = RP::template speed_other<decltype(P)::value>(roe);
+        finite = finite && isfinite(sp);
+        const double c1 = dtdy * sp, c2 = -dtdy * sp;
+        cflm = cflm > c1 ? cflm : c1;
+        cflm = cflm > c2 ? cflm : c2;
+    });
     return cflm;
 }
 

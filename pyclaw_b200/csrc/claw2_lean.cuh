@@ -280,13 +280,20 @@ __device__ __forceinline__ bool lean_uniform_halo(const StepArgs& a, const doubl
 {
     constexpr int MEQN = RP::MEQN;
     const int rmax = a.my + 3 - j0, cmax = a.mx + 3 - i0;   // last halo row / column inside the array
+    double q0[MEQN];
+#pragma unroll
+    for (int m = 0; m < MEQN; m++) q0[m] = H[lean_hidx<MEQN, TR>(m, 0, 0)];
     bool same = true;
-    for (int e = tid; e < TR * 32; e += nt) {
-        const int r = e >> 5, c = e & 31;
+    // columns c, c+1 (c even) sit side by side in the swizzled box: one
+    // 16-byte load per pair
+    for (int e = tid; e < TR * 16; e += nt) {
+        const int r = e >> 4, c = (e & 15) * 2;
         if (r <= rmax && c <= cmax) {
 #pragma unroll
-            for (int m = 0; m < MEQN; m++)
-                same = same && H[lean_hidx<MEQN, TR>(m, r, c)] == H[lean_hidx<MEQN, TR>(m, 0, 0)];
+            for (int m = 0; m < MEQN; m++) {
+                const double2 v = *reinterpret_cast<const double2*>(H + lean_hidx<MEQN, TR>(m, r, c));
+                same = same && v.x == q0[m] && (c + 1 > cmax || v.y == q0[m]);
+            }
         }
     }
     return __syncthreads_and(same);

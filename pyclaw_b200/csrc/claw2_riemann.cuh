@@ -246,6 +246,18 @@ template <bool TRACER> struct RpEuler {
         else if constexpr (P == 3) return roe[0] + roe[2];
         else return roe[0];
     }
+    // Between two equal states, speed of wave P of the other direction's
+    // solve from this direction's Roe averages: that solve's normal average
+    // is this one's transverse average v (the same operands and operations),
+    // and its sound speed is this one's a (the pressure and enthalpy do not
+    // depend on the direction, and u*u + v*v == v*v + u*u exactly).
+    template <int P>
+    static CLAW2_DEV double speed_other(const double (&roe)[NROE])
+    {
+        if constexpr (P == 0) return roe[1] - roe[2];
+        else if constexpr (P == 3) return roe[1] + roe[2];
+        else return roe[1];
+    }
     // rpn2c returning the wave strengths instead of the waves and speeds
     template <int IXY>
     static CLAW2_DEV void rpn2a(const double (&qL)[MEQN], const double (&qR)[MEQN], const Cell& L, const Cell& R,
@@ -518,6 +530,16 @@ struct RpShallow {
         if constexpr (P == 0) return roe[0] - roe[2];
         else if constexpr (P == 2) return roe[0] + roe[2];
         else return roe[0];
+    }
+    // Between two equal states, speed of wave P of the other direction's
+    // solve from this direction's Roe averages (see RpEuler::speed_other;
+    // cbar depends on the depths alone).
+    template <int P>
+    static CLAW2_DEV double speed_other(const double (&roe)[NROE])
+    {
+        if constexpr (P == 0) return roe[1] - roe[2];
+        else if constexpr (P == 2) return roe[1] + roe[2];
+        else return roe[1];
     }
     template <int IXY>
     static CLAW2_DEV void rpn2a(const double (&qL)[MEQN], const double (&qR)[MEQN], const Cell& L, const Cell& R,
