@@ -167,13 +167,11 @@ CLAW2_HD int ghost_images(int i, int n, int bl, int bu, int (&g)[2], bool (&neg)
     return k;
 }
 
-// Write one final cell value and all ghost cells that are images of it.
+// Write the ghost cells that are images of final cell (i, j) with value v
+// (ghost fill fused into the step).
 template <int MEQN>
-CLAW2_HD void write_cell(const StepArgs& a, double* qo, int i, int j, const double (&v)[MEQN])
+CLAW2_HD void write_ghosts(const StepArgs& a, double* qo, int i, int j, const double (&v)[MEQN])
 {
-#pragma unroll
-    for (int m = 0; m < MEQN; m++) qo[qoff(a, m, i, j)] = v[m];
-    if (!a.ghost_fused) return;
     int gx[2], gy[2];
     bool nx[2], ny[2];
     const int kx = ghost_images(i, a.mx, a.bcl[0], a.bcu[0], gx, nx);
@@ -621,19 +619,44 @@ CLAW2_HD void finish_tile(const StepArgs& a, Ctx& ctx, const TileId& tile, const
 {
     const int tid = ctx.tid();
     int bad = 0;
-    for (int idx = fault ? TX * TY : tid; idx < TX * TY; idx += NT) {
-        const int ci = idx % TX, cj = idx / TX;
-        const int i = i0 + ci, j = j0 + cj;
-        if (i >= a.mx || j >= a.my) continue;
-        double v[MEQN];
+    // the tile's final values: one unrolled pass of plain stores (the loads
+    // of all its cells issue together), then, on tiles within two cells of
+    // a side, a second pass writing the ghost cells that are images of them
+    constexpr int NIT = (TX * TY + NT - 1) / NT;
+    auto cell_value = [&](int ci, int cj, int i, int j, double (&v)[MEQN]) {
 #pragma unroll
         for (int m = 0; m < MEQN; m++) v[m] = Qx[m * QSTR + cj * QP + ci];
         if (a.src == CLAW2_SRC_EULER_RADIAL)
             euler_radial_source<MEQN>(v, a.aux[qoff(a, a.src_aux, i, j)], a.prm[1], dt);
+    };
+    if (!fault) {
 #pragma unroll
-        for (int m = 0; m < MEQN; m++)
-            if (!isfinite(v[m])) bad = 1;
-        write_cell<MEQN>(a, qout, i, j, v);
+        for (int k = 0; k < NIT; k++) {
+            const int idx = tid + k * NT;
+            const int ci = idx % TX, cj = idx / TX;
+            const int i = i0 + ci, j = j0 + cj;
+            if (idx < TX * TY && i < a.mx && j < a.my) {
+                double v[MEQN];
+                cell_value(ci, cj, i, j, v);
+#pragma unroll
+                for (int m = 0; m < MEQN; m++) {
+                    if (!isfinite(v[m])) bad = 1;
+                    qout[qoff(a, m, i, j)] = v[m];
+                }
+            }
+        }
+        const bool edge = i0 <= 1 || i0 + TX >= a.mx - 2 || j0 <= 1 || j0 + TY >= a.my - 2;
+        if (a.ghost_fused && edge) {
+            for (int idx = tid; idx < TX * TY; idx += NT) {
+                const int ci = idx % TX, cj = idx / TX;
+                const int i = i0 + ci, j = j0 + cj;
+                if (i >= a.mx || j >= a.my) continue;
+                if (i > 1 && i < a.mx - 2 && j > 1 && j < a.my - 2) continue;   // no images
+                double v[MEQN];
+                cell_value(ci, cj, i, j, v);
+                write_ghosts<MEQN>(a, qout, i, j, v);
+            }
+        }
     }
 
     // ---- block CFL max (deterministic: max is exact) and last-block epilogue:
