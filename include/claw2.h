@@ -384,6 +384,18 @@ CLAW2_EXPORT int claw2_batch_advance(const claw2_problem* p, const claw2_batch_i
  * claw2_graph_launch.  The descriptors and buffers must stay where they are. */
 CLAW2_EXPORT int claw2_batch_graph_create(const claw2_problem* p, const claw2_batch_instance* inst, int ninst,
                                           int ntiles, int nsteps, int variant, void** graph_exec);
+/* The same two with a tile -> instance map: tile_inst is a device array of
+ * ntiles int32, entry t the instance whose tiles include tile t.  The
+ * one-CTA-per-tile variants then find a tile's instance with one load
+ * instead of a binary search over the descriptors (an entry that does not
+ * hold its tile falls back to the search); the other variants ignore it.
+ * NULL means no map. */
+CLAW2_EXPORT int claw2_batch_advance_map(const claw2_problem* p, const claw2_batch_instance* inst, int ninst,
+                                         int ntiles, const int32_t* tile_inst, int nsteps, int variant,
+                                         void* stream);
+CLAW2_EXPORT int claw2_batch_graph_create_map(const claw2_problem* p, const claw2_batch_instance* inst, int ninst,
+                                              int ntiles, const int32_t* tile_inst, int nsteps, int variant,
+                                              void** graph_exec);
 CLAW2_EXPORT int claw2_graph_launch(void* graph_exec, void* stream);
 CLAW2_EXPORT int claw2_graph_destroy(void* graph_exec);
 

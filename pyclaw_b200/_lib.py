@@ -57,6 +57,10 @@ PROTOTYPES = [
     ("claw2_batch_advance", ctypes.c_int, [_P, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp]),
     ("claw2_batch_graph_create", ctypes.c_int, [_P, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                                 ctypes.POINTER(_vp)]),
+    ("claw2_batch_advance_map", ctypes.c_int, [_P, _vp, ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int, ctypes.c_int,
+                                               _vp]),
+    ("claw2_batch_graph_create_map", ctypes.c_int, [_P, _vp, ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int,
+                                                    ctypes.c_int, ctypes.POINTER(_vp)]),
     ("claw2_graph_launch", ctypes.c_int, [_vp, _vp]),
     ("claw2_graph_destroy", ctypes.c_int, [_vp]),
     ("claw2_session_create", ctypes.c_int, [_P, ctypes.POINTER(_vp)]),

@@ -121,6 +121,13 @@ class BatchSolver(object):
         self.desc_dev_of = {e: torch.frombuffer(bytearray(bytes(t)), dtype=torch.uint8).to(self.device)
                             for e, t in tables.items()}
         self.desc_dev = self.desc_dev_of[29]
+        # tile -> instance maps, one per tile edge (the one-CTA-per-tile
+        # variants read a tile's instance from it)
+        self.map_dev_of = {}
+        for e, t in tables.items():
+            counts = [t[k].nbx * t[k].nby for k in range(self.n)]
+            self.map_dev_of[e] = torch.from_numpy(
+                np.repeat(np.arange(self.n, dtype=np.int32), counts)).to(self.device)
         self.variant = 0
         self._graphs = {}
         self.tuning = None
@@ -184,13 +191,17 @@ class BatchSolver(object):
         e = self.tile_of[v]
         return self.desc_dev_of[e], self.ntiles_of[e]
 
+    def _map(self, v):
+        """Device tile -> instance map of variant v's edge."""
+        return ctypes.c_void_p(self.map_dev_of[self.tile_of[v]].data_ptr())
+
     def advance(self, nsteps, variant=None):
         """nsteps batched launches (no graph)."""
         v = self.variant if variant is None else variant
         desc, nt = self._table(v)
-        _lib.check(self.lib.claw2_batch_advance(ctypes.byref(self.p), ctypes.c_void_p(desc.data_ptr()),
-                                                self.n, nt, int(nsteps), int(v), self._stream()),
-                   "claw2_batch_advance")
+        _lib.check(self.lib.claw2_batch_advance_map(ctypes.byref(self.p), ctypes.c_void_p(desc.data_ptr()),
+                                                    self.n, nt, self._map(v), int(nsteps), int(v), self._stream()),
+                   "claw2_batch_advance_map")
 
     def advance_graph(self, nsteps, chunk=50):
         """nsteps launches replayed from CUDA graphs of `chunk` launches."""
@@ -202,9 +213,11 @@ class BatchSolver(object):
             if key not in self._graphs:
                 ge = ctypes.c_void_p()
                 desc, nt = self._table(self.variant)
-                _lib.check(self.lib.claw2_batch_graph_create(ctypes.byref(self.p), ctypes.c_void_p(desc.data_ptr()),
-                                                             self.n, nt, count, self.variant, ctypes.byref(ge)),
-                           "claw2_batch_graph_create")
+                _lib.check(self.lib.claw2_batch_graph_create_map(ctypes.byref(self.p),
+                                                                 ctypes.c_void_p(desc.data_ptr()), self.n, nt,
+                                                                 self._map(self.variant), count, self.variant,
+                                                                 ctypes.byref(ge)),
+                           "claw2_batch_graph_create_map")
                 self._graphs[key] = ge
             for _ in range(reps):
                 _lib.check(self.lib.claw2_graph_launch(self._graphs[key], self._stream()), "claw2_graph_launch")

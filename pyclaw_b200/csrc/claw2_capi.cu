@@ -212,18 +212,23 @@ batch_kernel(const claw2_batch_instance* __restrict__ inst, int ninst, int ntile
 // Batched step with one CTA per tile (grid = all tiles of all instances):
 // the hardware hands tiles to SMs as slots free up, so uneven tiles balance
 // themselves, and no loop state stays live across the tile body.  The tile's
-// instance comes from a binary search over the descriptors (their first
-// levels stay in L1 and L2 across CTAs); there is no L2 prefetch of a next
-// tile, the other resident CTAs cover the first loads.
+// instance comes from the caller's tile -> instance map when there is one,
+// else from a binary search over the descriptors (a chain of dependent L2
+// loads at the CTA's start); there is no L2 prefetch of a next tile, the
+// other resident CTAs cover the first loads.
 template <class RP, int NT, int MINB, bool LIGHT, int T>
 __global__ void __launch_bounds__(NT, MINB)
-batch_tile_kernel(const claw2_batch_instance* __restrict__ inst, int ninst, StepArgs common)
+batch_tile_kernel(const claw2_batch_instance* __restrict__ inst, int ninst, StepArgs common,
+                  const int32_t* __restrict__ tile_inst)
 {
     static_assert(LIGHT || T == 29, "the generic body runs 29x29 tiles in the batch");
     extern __shared__ double smem_dyn[];
     DevCtx ctx{smem_dyn};
     const int t = (int)blockIdx.x;
-    const claw2_batch_instance& I = inst[batch_instance_of(inst, ninst, t)];
+    int k = tile_inst ? __ldg(&tile_inst[t]) : -1;  // the caller's map: one load
+    if (k < 0 || k >= ninst || t < inst[k].tile_begin || t - inst[k].tile_begin >= inst[k].nbx * inst[k].nby)
+        k = batch_instance_of(inst, ninst, t);      // no map, or an entry that does not hold tile t
+    const claw2_batch_instance& I = inst[k];
     StepArgs a = common;
     a.q0 = I.q0; a.q1 = I.q1; a.aux = I.aux; a.ctrl = I.ctrl;
     a.partials = I.partials; a.ticket = I.ticket;
@@ -1045,14 +1050,14 @@ int batch_launch_t(const StepArgs& common, const claw2_batch_instance* inst, int
 
 template <class RP, int NT, int MINB, bool LIGHT, int T>
 int batch_launch_tiles(const StepArgs& common, const claw2_batch_instance* inst, int ninst, int ntiles, int nsteps,
-                       cudaStream_t st)
+                       const int32_t* tile_inst, cudaStream_t st)
 {
     constexpr int SMB = LIGHT ? LightSmem<T, T, NT>::bytes : TileSmem<RP, 29, 29, NT, false>::bytes;
     auto kern = batch_tile_kernel<RP, NT, MINB, LIGHT, T>;
     static std::atomic<uint64_t> optin{0};
     if (smem_optin(optin, kern, SMB) != cudaSuccess) return CLAW2_ERR_CUDA;
     for (int n = 0; n < nsteps; n++) {
-        kern<<<ntiles, NT, SMB, st>>>(inst, ninst, common);
+        kern<<<ntiles, NT, SMB, st>>>(inst, ninst, common, tile_inst);
         if (cudaGetLastError() != cudaSuccess) return CLAW2_ERR_CUDA;
     }
     return CLAW2_OK;
@@ -1060,7 +1065,7 @@ int batch_launch_tiles(const StepArgs& common, const claw2_batch_instance* inst,
 
 template <class RP>
 int batch_launch_rp(int variant, const StepArgs& c, const claw2_batch_instance* inst, int ninst, int ntiles,
-                    int nsteps, cudaStream_t st)
+                    int nsteps, const int32_t* tile_inst, cudaStream_t st)
 {
     if constexpr (HasLight<RP>::value) {
         if (c.capa < 0 && !c.fwave) {
@@ -1075,10 +1080,10 @@ int batch_launch_rp(int variant, const StepArgs& c, const claw2_batch_instance* 
             case 7: return batch_launch_t<RP, 256, 4, true, 21>(c, inst, ninst, ntiles, nsteps, st);
             case 8: return batch_launch_t<RP, 256, 3, true, 13>(c, inst, ninst, ntiles, nsteps, st);
             case 9: return batch_launch_t<RP, 256, 4, true, 13>(c, inst, ninst, ntiles, nsteps, st);
-            case 10: return batch_launch_tiles<RP, 256, 3, true, 29>(c, inst, ninst, ntiles, nsteps, st);
-            case 11: return batch_launch_tiles<RP, 256, 4, true, 29>(c, inst, ninst, ntiles, nsteps, st);
-            case 12: return batch_launch_tiles<RP, 128, 6, true, 29>(c, inst, ninst, ntiles, nsteps, st);
-            case 13: return batch_launch_tiles<RP, 512, 2, true, 29>(c, inst, ninst, ntiles, nsteps, st);
+            case 10: return batch_launch_tiles<RP, 256, 3, true, 29>(c, inst, ninst, ntiles, nsteps, tile_inst, st);
+            case 11: return batch_launch_tiles<RP, 256, 4, true, 29>(c, inst, ninst, ntiles, nsteps, tile_inst, st);
+            case 12: return batch_launch_tiles<RP, 128, 6, true, 29>(c, inst, ninst, ntiles, nsteps, tile_inst, st);
+            case 13: return batch_launch_tiles<RP, 512, 2, true, 29>(c, inst, ninst, ntiles, nsteps, tile_inst, st);
             default: return CLAW2_ERR_INVALID;
             }
         }
@@ -1093,7 +1098,7 @@ int batch_launch_rp(int variant, const StepArgs& c, const claw2_batch_instance* 
 }
 
 int batch_launch(const claw2_problem* p, const claw2_batch_instance* inst, int ninst, int ntiles, int nsteps,
-                 int variant, cudaStream_t st)
+                 int variant, const int32_t* tile_inst, cudaStream_t st)
 {
     StepArgs c;
     fill_args(p, nullptr, c);
@@ -1101,12 +1106,12 @@ int batch_launch(const claw2_problem* p, const claw2_batch_instance* inst, int n
     for (int d = 0; d < 2; d++)
         if (p->bc_lower[d] == CLAW2_BC_CUSTOM || p->bc_upper[d] == CLAW2_BC_CUSTOM) return CLAW2_ERR_UNSUPPORTED;
     switch (p->rp) {
-    case CLAW2_RP_ACOUSTICS: return batch_launch_rp<RpAcoustics>(variant, c, inst, ninst, ntiles, nsteps, st);
-    case CLAW2_RP_VC_ACOUSTICS: return batch_launch_rp<RpVcAcoustics>(variant, c, inst, ninst, ntiles, nsteps, st);
-    case CLAW2_RP_EULER_4WAVE: return batch_launch_rp<RpEuler<false>>(variant, c, inst, ninst, ntiles, nsteps, st);
-    case CLAW2_RP_EULER_5WAVE: return batch_launch_rp<RpEuler<true>>(variant, c, inst, ninst, ntiles, nsteps, st);
-    case CLAW2_RP_SHALLOW_ROE: return batch_launch_rp<RpShallow>(variant, c, inst, ninst, ntiles, nsteps, st);
-    case CLAW2_RP_PSYSTEM: return batch_launch_rp<RpPsystem>(variant, c, inst, ninst, ntiles, nsteps, st);
+    case CLAW2_RP_ACOUSTICS: return batch_launch_rp<RpAcoustics>(variant, c, inst, ninst, ntiles, nsteps, tile_inst, st);
+    case CLAW2_RP_VC_ACOUSTICS: return batch_launch_rp<RpVcAcoustics>(variant, c, inst, ninst, ntiles, nsteps, tile_inst, st);
+    case CLAW2_RP_EULER_4WAVE: return batch_launch_rp<RpEuler<false>>(variant, c, inst, ninst, ntiles, nsteps, tile_inst, st);
+    case CLAW2_RP_EULER_5WAVE: return batch_launch_rp<RpEuler<true>>(variant, c, inst, ninst, ntiles, nsteps, tile_inst, st);
+    case CLAW2_RP_SHALLOW_ROE: return batch_launch_rp<RpShallow>(variant, c, inst, ninst, ntiles, nsteps, tile_inst, st);
+    case CLAW2_RP_PSYSTEM: return batch_launch_rp<RpPsystem>(variant, c, inst, ninst, ntiles, nsteps, tile_inst, st);
     default: return CLAW2_ERR_INVALID;
     }
 }
@@ -1161,13 +1166,25 @@ int claw2_batch_tiles_for(int tile, int mx, int my, int* nbx, int* nby)
 int claw2_batch_advance(const claw2_problem* p, const claw2_batch_instance* inst, int ninst, int ntiles, int nsteps,
                         int variant, void* stream)
 {
+    return claw2_batch_advance_map(p, inst, ninst, ntiles, nullptr, nsteps, variant, stream);
+}
+
+int claw2_batch_advance_map(const claw2_problem* p, const claw2_batch_instance* inst, int ninst, int ntiles,
+                            const int32_t* tile_inst, int nsteps, int variant, void* stream)
+{
     int rc = batch_check(p, inst, ninst, ntiles, nsteps, variant);
     if (rc) return rc;
-    return batch_launch(p, inst, ninst, ntiles, nsteps, variant, S(stream));
+    return batch_launch(p, inst, ninst, ntiles, nsteps, variant, tile_inst, S(stream));
 }
 
 int claw2_batch_graph_create(const claw2_problem* p, const claw2_batch_instance* inst, int ninst, int ntiles,
                              int nsteps, int variant, void** graph_exec)
+{
+    return claw2_batch_graph_create_map(p, inst, ninst, ntiles, nullptr, nsteps, variant, graph_exec);
+}
+
+int claw2_batch_graph_create_map(const claw2_problem* p, const claw2_batch_instance* inst, int ninst, int ntiles,
+                                 const int32_t* tile_inst, int nsteps, int variant, void** graph_exec)
 {
     int rc = batch_check(p, inst, ninst, ntiles, nsteps, variant);
     if (rc) return rc;
@@ -1176,12 +1193,12 @@ int claw2_batch_graph_create(const claw2_problem* p, const claw2_batch_instance*
     // attribute, occupancy) so that the capture itself only records launches
     cudaStream_t st;
     if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) return CLAW2_ERR_CUDA;
-    rc = batch_launch(p, inst, ninst, ntiles, 0, variant, st);
+    rc = batch_launch(p, inst, ninst, ntiles, 0, variant, tile_inst, st);
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     if (!rc && cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) rc = CLAW2_ERR_CUDA;
     if (!rc) {
-        const int r2 = batch_launch(p, inst, ninst, ntiles, nsteps, variant, st);
+        const int r2 = batch_launch(p, inst, ninst, ntiles, nsteps, variant, tile_inst, st);
         if (cudaStreamEndCapture(st, &graph) != cudaSuccess || r2) rc = r2 ? r2 : CLAW2_ERR_CUDA;
     }
     if (!rc && cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess) rc = CLAW2_ERR_CUDA;

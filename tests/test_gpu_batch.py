@@ -127,3 +127,31 @@ def test_batched_euler_one_state_tiles_equal_single_runs():
         assert ctrls[k].numsteps == c_alone.numsteps and ctrls[k].t == c_alone.t and ctrls[k].dt == c_alone.dt
         assert np.array_equal(bs.solution(k), q_alone)
     bs.close()
+
+
+def test_tile_map_and_search_give_the_same_batch():
+    """The one-CTA-per-tile variants read a tile's instance from the
+    BatchSolver's tile -> instance map (claw2_batch_advance_map); without a
+    map (claw2_batch_advance) they search the descriptors.  Both must give the
+    same states, bit for bit."""
+    prob, insts = bench.batched_vc_config(n=9, seed=11, nmin=40, nmax=130)
+    from pyclaw_b200.batch import BatchSolver
+    lib = _lib.load()
+    nv = lib.claw2_batch_num_variants()
+    per_tile = [v for v in range(nv) if v >= 10]
+    assert per_tile
+    for v in per_tile:
+        sols = []
+        for mapped in (True, False):
+            bs = BatchSolver(prob, insts)
+            bs.init_controls([i["dt"] for i in insts], max_steps=12)
+            if mapped:
+                bs.advance(12, v)
+            else:
+                desc, nt = bs._table(v)
+                _lib.check(lib.claw2_batch_advance(ctypes.byref(bs.p), ctypes.c_void_p(desc.data_ptr()), bs.n, nt,
+                                                   12, v, bs._stream()), "claw2_batch_advance")
+            sols.append([bs.solution(k) for k in range(len(insts))])
+            bs.close()
+        for a, b in zip(*sols):
+            assert np.array_equal(a, b)
