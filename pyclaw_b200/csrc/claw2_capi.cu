@@ -26,9 +26,45 @@ namespace claw2 {
 #define CLAW2_MINB 2        // resident CTAs per SM the register budget is sized for
 #endif
 
+// Chained steps (launch_step with chained set): once every CTA of this step
+// has started, the next step's CTAs may start on the SMs this step frees;
+// each waits here until the step before it has completed and its writes are
+// visible.  In a kernel launched without the attribute both instructions
+// return at once.
+__device__ __forceinline__ void chain_wait()
+{
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
+// Launch kern, as a programmatic dependent of the previous kernel in the
+// stream when chained is set (the kernel calls chain_wait before it reads
+// anything).
+template <class... KArgs, class... Args>
+int launch_kernel(void (*kern)(KArgs...), dim3 grid, int threads, int smem, cudaStream_t st, bool chained,
+                  Args... args)
+{
+    if (!chained) {
+        kern<<<grid, threads, smem, st>>>(args...);
+        return cudaGetLastError() == cudaSuccess ? CLAW2_OK : CLAW2_ERR_CUDA;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = dim3(threads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kern, args...) == cudaSuccess ? CLAW2_OK : CLAW2_ERR_CUDA;
+}
+
 template <class RP, int TX, int TY, int NT, bool SPLIT>
 __global__ void __launch_bounds__(NT, CLAW2_MINB) step_kernel(StepArgs a)
 {
+    chain_wait();
     extern __shared__ double smem_dyn[];
     DevCtx ctx{smem_dyn};
     step_tile<RP, TX, TY, NT, SPLIT>(a, ctx);
@@ -57,6 +93,7 @@ CLAW2_HD bool light_small_grid(int mx, int my)
 template <class RP, int T>
 __global__ void __launch_bounds__(256, CLAW2_LIGHT_MINB) light_step_kernel(StepArgs a)
 {
+    chain_wait();
     extern __shared__ double smem_dyn[];
     DevCtx ctx{smem_dyn};
     const TileId t{(int)blockIdx.x, (int)blockIdx.y, (int)gridDim.x, (int)gridDim.y,
@@ -90,13 +127,7 @@ lean_step_kernel(StepArgs a, const __grid_constant__ CUtensorMap tm0, const __gr
 {
     extern __shared__ double smem_dyn[];
     __shared__ __align__(8) uint64_t halo_bar;
-    // Chained steps (launch_lean_t with chained set): once every CTA of this
-    // step has started, the next step's CTAs may start on the SMs this step
-    // frees and wait here until this step has completed and its writes are
-    // visible.  Launched without the attribute both instructions return at
-    // once.
-    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-    asm volatile("griddepcontrol.wait;" ::: "memory");
+    chain_wait();
     DevCtx ctx{smem_dyn};
     const TileId t{(int)blockIdx.x, (int)blockIdx.y, (int)gridDim.x, (int)gridDim.y,
                    (int)(blockIdx.y * gridDim.x + blockIdx.x), (int)(gridDim.x * gridDim.y)};
@@ -510,22 +541,21 @@ void fill_args(const claw2_problem* p, double* q, StepArgs& a)
 }
 
 template <class RP, int T>
-int launch_light_t(const StepArgs& a, int nbx, int nby, cudaStream_t st)
+int launch_light_t(const StepArgs& a, int nbx, int nby, cudaStream_t st, bool chained)
 {
     using SM = LightSmem<T, T, 256>;
     auto kern = light_step_kernel<RP, T>;
     static std::atomic<uint64_t> optin{0};
     if (smem_optin(optin, kern, SM::bytes) != cudaSuccess) return CLAW2_ERR_CUDA;
-    kern<<<dim3(nbx, nby), 256, SM::bytes, st>>>(a);
-    return cudaGetLastError() == cudaSuccess ? CLAW2_OK : CLAW2_ERR_CUDA;
+    return launch_kernel(kern, dim3(nbx, nby), 256, SM::bytes, st, chained, a);
 }
 
 // nbx x nby come from tiles(), which makes the same choice
 template <class RP>
-int launch_light(const StepArgs& a, int nbx, int nby, cudaStream_t st)
+int launch_light(const StepArgs& a, int nbx, int nby, cudaStream_t st, bool chained)
 {
-    if (light_small_grid(a.mx, a.my)) return launch_light_t<RP, LIGHT_SMALL_TILE>(a, nbx, nby, st);
-    return launch_light_t<RP, 29>(a, nbx, nby, st);
+    if (light_small_grid(a.mx, a.my)) return launch_light_t<RP, LIGHT_SMALL_TILE>(a, nbx, nby, st, chained);
+    return launch_light_t<RP, 29>(a, nbx, nby, st, chained);
 }
 
 // cuTensorMapEncodeTiled from the driver, found through the runtime (no link
@@ -568,8 +598,7 @@ int halo_tensor_map(CUtensorMap* m, const double* q, const StepArgs& a, int meqn
 std::atomic<int> g_halo_shortfall{0};
 
 // chained: the previous operation in the stream is a step kernel of the same
-// device loop, so this launch may overlap its end (programmatic dependent
-// launch; the kernel waits for it before reading anything).
+// device loop (launch_kernel).
 template <class RP, int NT>
 int launch_lean_t(const StepArgs& a0, int nbx, int nby, cudaStream_t st, bool chained)
 {
@@ -583,21 +612,7 @@ int launch_lean_t(const StepArgs& a0, int nbx, int nby, cudaStream_t st, bool ch
     int rc = halo_tensor_map(&tm0, a.ctrl ? a.q0 : a.qin, a, RP::MEQN);
     if (!rc) rc = a.ctrl ? halo_tensor_map(&tm1, a.q1, a, RP::MEQN) : (tm1 = tm0, CLAW2_OK);
     if (rc) return rc;
-    if (!chained) {
-        kern<<<dim3(nbx, nby), NT, SM::bytes, st>>>(a, tm0, tm1);
-        return cudaGetLastError() == cudaSuccess ? CLAW2_OK : CLAW2_ERR_CUDA;
-    }
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(nbx, nby);
-    cfg.blockDim = dim3(NT);
-    cfg.dynamicSmemBytes = SM::bytes;
-    cfg.stream = st;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    attr[0].val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, kern, a, tm0, tm1) == cudaSuccess ? CLAW2_OK : CLAW2_ERR_CUDA;
+    return launch_kernel(kern, dim3(nbx, nby), NT, SM::bytes, st, chained, a, tm0, tm1);
 }
 
 template <class RP>
@@ -611,7 +626,7 @@ template <class RP, bool SPLIT>
 int launch_step_t(const StepArgs& a, int nbx, int nby, cudaStream_t st, bool chained)
 {
     if constexpr (!SPLIT && HasLight<RP>::value)
-        if (a.capa < 0 && !a.fwave) return launch_light<RP>(a, nbx, nby, st);
+        if (a.capa < 0 && !a.fwave) return launch_light<RP>(a, nbx, nby, st, chained);
     if constexpr (!SPLIT && HasLean<RP>::value)
         if (a.capa < 0 && !a.fwave) return launch_lean<RP>(a, nbx, nby, st, chained);
     constexpr int TX = SPLIT ? STX : UTX, TY = SPLIT ? STY : UTY, NT = SPLIT ? SNT : UNT;
@@ -619,11 +634,11 @@ int launch_step_t(const StepArgs& a, int nbx, int nby, cudaStream_t st, bool cha
     auto kern = step_kernel<RP, TX, TY, NT, SPLIT>;
     static std::atomic<uint64_t> optin{0};
     if (smem_optin(optin, kern, SM::bytes) != cudaSuccess) return CLAW2_ERR_CUDA;
-    kern<<<dim3(nbx, nby), NT, SM::bytes, st>>>(a);
-    return cudaGetLastError() == cudaSuccess ? CLAW2_OK : CLAW2_ERR_CUDA;
+    return launch_kernel(kern, dim3(nbx, nby), NT, SM::bytes, st, chained, a);
 }
 
-// chained: see launch_lean_t (only the lean body takes it up).
+// chained: the previous operation in the stream is a step kernel of the same
+// device loop, so this step may overlap its end (launch_kernel).
 int launch_step(const claw2_problem* p, const StepArgs& a, cudaStream_t st, bool chained = false)
 {
     int nbx, nby;

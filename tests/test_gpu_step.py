@@ -324,21 +324,29 @@ def test_all_uniform_grid_keeps_its_state_and_cfl(orc, name):
 
 
 
-@pytest.mark.parametrize("name,mx,my", [("euler4", 140, 84), ("shallow", 1010, 1000)])
-def test_chained_steps_equal_single_step_calls(name, mx, my):
-    """claw2_advance launches the lean body's steps after its first as
-    programmatic dependents of the step before; 30 steps in one call must
-    leave the state, t and dt bit for bit where 30 calls of one step do."""
+@pytest.mark.parametrize("name,mx,my,tr", [("euler4", 140, 84, 2), ("shallow", 1010, 1000, 2),
+                                          ("acoustics", 120, 90, 2), ("vc_acoustics", 500, 460, 2),
+                                          ("euler4", 140, 84, -1)])
+def test_chained_steps_equal_single_step_calls(name, mx, my, tr):
+    """claw2_advance launches each step after its first as a programmatic
+    dependent of the step before (lean, light and generic bodies); 30 steps in
+    one call must leave the state, t and dt bit for bit where 30 calls of one
+    step do."""
     import ctypes
     from pyclaw_b200 import _abi, _lib
     from pyclaw_b200.device import DeviceState
     t = H.torch()
     lib = _lib.load()
-    p = H.problem(name, mx, my, 2, bcl=(1, 3), bcu=(3, 1))
-    q = _piecewise_uniform(p, "moving", seed=9)
+    p = H.problem(name, mx, my, tr, bcl=(1, 3), bcu=(3, 1))
+    if p.rp in (_abi.RP_ACOUSTICS, _abi.RP_VC_ACOUSTICS):
+        q, aux = H.init_fields(p, seed=9)
+    else:
+        q, aux = _piecewise_uniform(p, "moving", seed=9), None
     results = []
     for calls in (1, 30):
         dev = DeviceState(p)
+        if aux is not None:
+            dev.upload_aux(aux)
         dev.upload_q(q)
         c = _abi.Control.from_address(dev.ctrl_host.data_ptr())
         _lib.check(lib.claw2_control_init(ctypes.byref(c), 0.0, 0.2 / max(mx, my), 1e9, 1.0, 0.9, 1e99, 1, 0,
