@@ -156,7 +156,7 @@ class DeviceState(object):
         g.cells, g.record, g.state = (self._g_cells.data_ptr(), self._g_record.data_ptr(), self._g_state.data_ptr())
         return g
 
-    def evolve(self, control, max_batch=64, hooks=None, gauges=None, on_gauges=None):
+    def evolve(self, control, max_batch=256, hooks=None, gauges=None, on_gauges=None):
         """Run the device-controlled loop until control is done; returns the
         final Control.  hooks: a claw2_hooks (source term run on the device).
         gauges: a list of interior cells (ix, iy) sampled after every accepted
@@ -172,7 +172,15 @@ class DeviceState(object):
         if gauges:
             rec = self.gauge_recorder(gauges, max_batch)
             self._g_state[1] = int(control.numsteps)
-        batch = 8
+        # each batch is the controller's estimate of the steps left (the
+        # host reads the controller only between batches; steps launched
+        # after it is done return at once)
+        def estimate():
+            left = max(1, int(host.max_steps - host.iter))       # loop iterations the controller allows
+            if host.dt > 0:
+                left = min(left, (host.tend - host.t) / host.dt + 1)
+            return int(max(1, min(max_batch, left)))
+        batch = estimate()
         while True:
             if rec is not None:
                 _lib.check(self.lib.claw2_advance_gauged(ctypes.byref(self.p), self.ptr(self.q[0]),
@@ -202,11 +210,7 @@ class DeviceState(object):
             stream.synchronize()
             if host.done:
                 break
-            if host.dt > 0:
-                remaining = (host.tend - host.t) / host.dt
-                batch = int(max(1, min(max_batch, remaining + 1)))
-            else:
-                batch = max_batch
+            batch = estimate()
         out = _abi.Control()
         ctypes.memmove(ctypes.addressof(out), ctypes.addressof(host), ctypes.sizeof(out))
         self.cur = out.cur
