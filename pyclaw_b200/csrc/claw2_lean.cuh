@@ -23,7 +23,10 @@
 //    is staged in shared memory once by the tensor memory accelerator (two
 //    boxes of 16 columns x 32 rows x MEQN fields, 128-byte swizzle; see
 //    claw2_tma.cuh) while the threads wait on an mbarrier; x lines read rows
-//    of it and y lines read down its columns.
+//    of it and y lines read down its columns;
+//  - a tile whose staged halo holds one state skips both sweeps: every
+//    interface would join two equal states, so its cells keep their values
+//    and its CFL number comes from one Riemann solve (uniform_cfl).
 #pragma once
 
 #include "claw2_kernels.cuh"
