@@ -6,6 +6,7 @@
 #include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <atomic>
 #include <cmath>
 #include <cstdint>
@@ -1390,8 +1391,15 @@ int claw2_session_evolve(claw2_session* s, double* q, const double* aux, double*
         return rc;
     if (cudaMemcpyAsync(s->ctrl, s->ctrl_host, sizeof(claw2_control), cudaMemcpyHostToDevice, s->stream) != cudaSuccess)
         return CLAW2_ERR_CUDA;
-    const int batch = 16;
     for (;;) {
+        // the controller's own estimate of the steps left (to tend and to
+        // max_steps), at most 256 per batch: the host reads the controller
+        // only between batches, and steps launched after it is done return
+        // at once
+        const claw2_control* h = s->ctrl_host;
+        double left = (double)(h->max_steps - h->iter);
+        if (h->dt > 0.0) left = std::min(left, (h->tend - h->t) / h->dt + 1.0);
+        const int batch = (int)std::max(1.0, std::min(256.0, left));
         if ((rc = claw2_advance(p, s->q0, s->q1, s->aux, s->ctrl, s->scratch, batch, s->stream))) return rc;
         if (cudaMemcpyAsync(s->ctrl_host, s->ctrl, sizeof(claw2_control), cudaMemcpyDeviceToHost, s->stream) != cudaSuccess)
             return CLAW2_ERR_CUDA;

@@ -463,3 +463,37 @@ def test_psystem_fwave_app_matches_reference_gauges(orc, tmp_path):
     for gd, gh in zip(state.gauge_data, state_h.gauge_data):
         assert np.array_equal(gd, gh)
     assert np.array_equal(state.q, state_h.q)
+
+
+def test_session_evolve_host_buffers_matches_oracle(orc):
+    """claw2_session_evolve, the host-buffer form of one Controller.run output
+    interval (state up, the interval's steps under the device controller in
+    batches sized by its own estimate, state down), over two intervals: the
+    same state, t, dt and step count as the oracle's evolve_to_time."""
+    import ctypes
+    import gpu_helpers as H
+    from pyclaw_b200 import _lib
+    lib = _lib.load()
+    p = H.problem("euler4", 97, 61, 2, bcl=(1, 3), bcu=(1, 3))
+    q, _ = H.init_fields(p, seed=21)
+    dt0 = 0.3 / 97
+    ref = orc.Run(p, q, None, cfl_max=1.0, cfl_desired=0.9, dt_initial=dt0)
+    s = ctypes.c_void_p()
+    _lib.check(lib.claw2_session_create(ctypes.byref(p), ctypes.byref(s)), "session_create")
+    try:
+        host = np.asfortranarray(q.copy())
+        t = ctypes.c_double(0.0)
+        dt = ctypes.c_double(dt0)
+        status = (ctypes.c_double * 5)()
+        steps = 0
+        for tend in (0.05, 0.12):
+            _lib.check(lib.claw2_session_evolve(s, host.ctypes.data, None, ctypes.byref(t), ctypes.byref(dt), tend,
+                                                1.0, 0.9, 1e99, 100000, status), "session_evolve")
+            steps += int(status[3])
+            ref.evolve_to_time(tend)
+            assert t.value == ref.t == tend
+            assert np.array_equal(host, ref.q)
+        assert dt.value == ref.dt
+        assert steps == ref.steps_taken and steps > 40
+    finally:
+        lib.claw2_session_destroy(s)
